@@ -1,0 +1,77 @@
+// The Index interface (reference: nsparse/index.h:21-68). Search runs on the
+// GPU; `distances` and `labels` are caller-owned n*k arrays, row-major, padded
+// with (-1.0, -1) where fewer than k results exist.
+#ifndef NSPARSE_B200_INDEX_H
+#define NSPARSE_B200_INDEX_H
+
+#include <array>
+#include <cstddef>
+#include <cstdint>
+
+#include "nsparse/id_selector.h"
+#include "nsparse/types.h"
+
+namespace nsparse {
+
+// Engine knobs with no counterpart in the reference. `plain` runs one kernel
+// launch per query (the per-query baseline); the default batches every query
+// of a call into one persistent launch. warps_per_block = 0 lets the engine
+// choose.
+struct EngineOptions {
+    bool plain = false;
+    int warps_per_block = 0;
+};
+
+struct SearchParameters {
+    virtual ~SearchParameters() = default;
+    const IDSelector* get_id_selector() const { return id_selector; }
+    void set_id_selector(IDSelector* selector) { id_selector = selector; }
+    EngineOptions engine;
+
+private:
+    IDSelector* id_selector = nullptr;
+};
+
+// Work counters and device time of the calling thread's last search.
+struct SearchStats {
+    uint64_t docs_scored = 0;
+    uint64_t blocks_visited = 0;
+    uint64_t bytes = 0;          // algorithmic bytes the kernels read
+    uint64_t lists_probed = 0;
+    float kernel_ms = 0.0f;
+    int launches = 0;
+};
+const SearchStats& last_search_stats();
+
+class Index {
+public:
+    explicit Index(int dim = 0);
+    virtual ~Index() = default;
+    virtual std::array<char, 4> id() const = 0;
+    virtual void add(idx_t n, const idx_t* indptr, const term_t* indices,
+                     const float* values) = 0;
+    virtual void build();
+    virtual void search(idx_t n, const idx_t* indptr, const term_t* indices,
+                        const float* values, int k, float* distances, idx_t* labels,
+                        SearchParameters* search_parameters = nullptr);
+
+    int get_dimension() const { return dimension_; }
+    virtual size_t num_vectors() const = 0;
+    virtual void add_with_ids(idx_t n, const idx_t* indptr, const term_t* indices,
+                              const float* values, const idx_t* ids);
+
+    // File layout: int64 header (rows, cols, nnz), then int64 indptr
+    // (rows + 1 entries), int32 indices and float32 values (nnz each).
+    virtual void read_csr(const char* file_path, Residency residency = Residency::kInMemory);
+
+protected:
+    // Called by search() after argument validation.
+    virtual void search_impl(idx_t n, const idx_t* indptr, const term_t* indices,
+                             const float* values, int k, float* distances, idx_t* labels,
+                             SearchParameters* search_parameters) = 0;
+    int dimension_;
+};
+
+}  // namespace nsparse
+
+#endif

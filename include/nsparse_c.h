@@ -1,0 +1,158 @@
+/*
+ * C ABI of libnsparse_b200.so: the nsparse Index API for foreign-function
+ * callers (ctypes, cgo, JNI, N-API). Plain pointers and sizes only; no call
+ * throws across the boundary. Every function returns an nsp_status_t; on
+ * failure nsp_last_error() holds the message for the calling thread.
+ *
+ * Status codes map to the reference's exception types, which its SWIG layer
+ * turns into Python exceptions (nsparse/python/swignsparse.swig:47-59):
+ *   NSP_ERR_INVALID_ARGUMENT  std::invalid_argument -> ValueError
+ *   NSP_ERR_OUT_OF_RANGE      std::out_of_range     -> IndexError
+ *   NSP_ERR_NO_MEMORY         std::bad_alloc        -> MemoryError
+ *   NSP_ERR_RUNTIME           std::runtime_error    -> RuntimeError
+ *                             (CUDA failures included)
+ *
+ * Each entry point names the reference interface it replaces (paths inside
+ * the reference project).
+ */
+#ifndef NSPARSE_C_H
+#define NSPARSE_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    NSP_OK = 0,
+    NSP_ERR_INVALID_ARGUMENT = 1,
+    NSP_ERR_RUNTIME = 2,
+    NSP_ERR_OUT_OF_RANGE = 3,
+    NSP_ERR_NO_MEMORY = 4
+} nsp_status_t;
+
+typedef struct nsp_index nsp_index_t;           /* nsparse::Index* (owned) */
+typedef struct nsp_id_selector nsp_id_selector_t; /* nsparse::IDSelector* (owned) */
+typedef struct nsp_search_params nsp_search_params_t; /* nsparse::SearchParameters* (owned) */
+
+/* Message of the calling thread's last failure ("" if none). */
+const char* nsp_last_error(void);
+
+/* ---- index lifecycle -------------------------------------------------- */
+
+/* index_factory (nsparse/index_factory.h:16, index_factory.cpp:63-153).
+ * Caller owns *out; release with nsp_index_free. */
+nsp_status_t nsp_index_factory(int dim, const char* description, nsp_index_t** out);
+
+/* delete Index* (SWIG %newobject ownership, swignsparse.swig:178-189). */
+nsp_status_t nsp_index_free(nsp_index_t* index);
+
+/* Index::add (nsparse/index.h:34-35): n rows of CSR, int32 indptr[n+1],
+ * uint16 indices and float32 values of indptr[n] entries. */
+nsp_status_t nsp_index_add(nsp_index_t* index, int32_t n, const int32_t* indptr,
+                           const uint16_t* indices, const float* values);
+
+/* Index::add_with_ids (nsparse/index.h:52-54; IDMapIndex, id_map_index.cpp:70-80). */
+nsp_status_t nsp_index_add_with_ids(nsp_index_t* index, int32_t n, const int32_t* indptr,
+                                    const uint16_t* indices, const float* values,
+                                    const int32_t* ids);
+
+/* Index::build (nsparse/index.h:36). SEISMIC indexes build on the GPU. */
+nsp_status_t nsp_index_build(nsp_index_t* index);
+
+/* Index::search (nsparse/index.h:37-40, index.cpp:32-49; SWIG search_c /
+ * search_with_params, swignsparse.swig:149-163). distances/labels are
+ * caller-owned n*k arrays, row-major, padded with (-1.0, -1). params may be
+ * NULL. Host buffers; the copies to and from the GPU happen inside. */
+nsp_status_t nsp_index_search(nsp_index_t* index, int32_t n, const int32_t* indptr,
+                              const uint16_t* indices, const float* values, int k,
+                              float* distances, int32_t* labels,
+                              const nsp_search_params_t* params);
+
+/* Index::num_vectors (nsparse/index.h:45-48). */
+nsp_status_t nsp_index_num_vectors(const nsp_index_t* index, int64_t* out);
+
+/* Index::get_dimension (nsparse/index.h:43). */
+nsp_status_t nsp_index_dimension(const nsp_index_t* index, int32_t* out);
+
+/* Index::id (nsparse/index.h:33): four characters, not NUL-terminated. */
+nsp_status_t nsp_index_fourcc(const nsp_index_t* index, char out[4]);
+
+/* Index::read_csr (nsparse/index.h:56-58, index.cpp:63-142). residency:
+ * 0 in-memory, 1 mmap (accepted; the index is copied to the GPU either way). */
+nsp_status_t nsp_index_read_csr(nsp_index_t* index, const char* path, int residency);
+
+/* write_index / read_index (nsparse/io/index_io.h:29-32). io_flags: 1 =
+ * kUseMmap (accepted). The file layout is the reference's. */
+nsp_status_t nsp_write_index(nsp_index_t* index, const char* path);
+nsp_status_t nsp_read_index(const char* path, int io_flags, nsp_index_t** out);
+
+/* ---- id selectors (nsparse/id_selector.h:22-86) ------------------------ */
+
+nsp_status_t nsp_id_selector_set_new(size_t n, const int32_t* ids, nsp_id_selector_t** out);
+nsp_status_t nsp_id_selector_array_new(size_t n, const int32_t* ids, nsp_id_selector_t** out);
+/* NotIDSelector borrows `inner`, which must outlive it (as in the reference). */
+nsp_status_t nsp_id_selector_not_new(nsp_id_selector_t* inner, nsp_id_selector_t** out);
+/* Extension with no counterpart in the reference: a ready-made membership
+ * bitmap over ids [0, n_bits), bit d of word d/64; the bits are copied. */
+nsp_status_t nsp_id_selector_bitmap_new(int64_t n_bits, const uint64_t* bits,
+                                        nsp_id_selector_t** out);
+nsp_status_t nsp_id_selector_is_member(const nsp_id_selector_t* sel, int32_t id, int* out);
+nsp_status_t nsp_id_selector_free(nsp_id_selector_t* sel);
+
+/* ---- search parameters ------------------------------------------------- */
+
+/* SearchParameters (nsparse/index.h:21-28). */
+nsp_status_t nsp_search_params_new(nsp_search_params_t** out);
+/* SeismicSearchParameters(cut, heap_factor) (nsparse/seismic_index.h:26-32). */
+nsp_status_t nsp_seismic_search_params_new(int cut, float heap_factor,
+                                           nsp_search_params_t** out);
+/* SeismicSQSearchParameters(vmin, vmax, cut, heap_factor)
+ * (nsparse/seismic_scalar_quantized_index.h:27-33). */
+nsp_status_t nsp_seismic_sq_search_params_new(float vmin, float vmax, int cut,
+                                              float heap_factor, nsp_search_params_t** out);
+/* SearchParameters::set_id_selector (borrowed; NULL clears). */
+nsp_status_t nsp_search_params_set_id_selector(nsp_search_params_t* params,
+                                               nsp_id_selector_t* sel);
+/* Extension: plain = 1 runs one kernel launch per query instead of one
+ * batched launch; warps_per_block = 0 lets the engine choose. */
+nsp_status_t nsp_search_params_set_engine(nsp_search_params_t* params, int plain,
+                                          int warps_per_block);
+nsp_status_t nsp_search_params_free(nsp_search_params_t* params);
+
+/* ---- engine extensions -------------------------------------------------- */
+
+typedef struct {
+    uint64_t docs_scored;
+    uint64_t blocks_visited;
+    uint64_t bytes;        /* algorithmic bytes the search kernels read */
+    uint64_t lists_probed;
+    float kernel_ms;       /* device time of the search kernels */
+    int32_t launches;
+} nsp_search_stats_t;
+
+/* Counters of the calling thread's last nsp_index_search. */
+nsp_status_t nsp_last_search_stats(nsp_search_stats_t* out);
+
+/* SEISMIC search with queries and results already in device memory (no host
+ * copies): d_indptr/d_indices/d_values describe n canonical query rows (terms
+ * ascending and unique within a row), max_row_nnz bounds the row length.
+ * d_distances/d_labels receive n*k results. Runs on `cuda_stream`
+ * (cudaStream_t, NULL = the thread's engine stream) and returns once the work
+ * is enqueued. Extension with no counterpart in the reference. */
+nsp_status_t nsp_index_search_device(nsp_index_t* index, int32_t n, const int32_t* d_indptr,
+                                     const uint16_t* d_indices, const float* d_values,
+                                     int32_t max_row_nnz, int k, float* d_distances,
+                                     int32_t* d_labels, const nsp_search_params_t* params,
+                                     void* cuda_stream);
+
+/* Number of CUDA devices visible and the name of the current one. */
+nsp_status_t nsp_device_info(int32_t* n_devices, char* name, size_t name_len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NSPARSE_C_H */

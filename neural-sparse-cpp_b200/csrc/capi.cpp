@@ -1,0 +1,284 @@
+// C ABI over the nsparse C++ API (include/nsparse_c.h). Exceptions are caught
+// here and mapped to status codes; the message is kept per thread.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+
+#include "engine.h"
+#include "index_state.h"
+#include "nsparse/brutal_index.h"
+#include "nsparse/id_map_index.h"
+#include "nsparse/index_factory.h"
+#include "nsparse/inverted_index.h"
+#include "nsparse/io/index_io.h"
+#include "nsparse/seismic_index.h"
+#include "nsparse/seismic_scalar_quantized_index.h"
+#include "nsparse_c.h"
+
+using namespace nsparse;
+
+namespace {
+
+thread_local std::string g_error;
+
+template <class F>
+nsp_status_t guarded(F&& f) {
+    try {
+        g_error.clear();
+        f();
+        return NSP_OK;
+    } catch (const std::invalid_argument& e) {
+        g_error = e.what();
+        return NSP_ERR_INVALID_ARGUMENT;
+    } catch (const std::out_of_range& e) {
+        g_error = e.what();
+        return NSP_ERR_OUT_OF_RANGE;
+    } catch (const std::bad_alloc& e) {
+        g_error = e.what();
+        return NSP_ERR_NO_MEMORY;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return NSP_ERR_RUNTIME;
+    } catch (...) {
+        g_error = "unknown error";
+        return NSP_ERR_RUNTIME;
+    }
+}
+
+Index* as_index(nsp_index_t* p) {
+    if (p == nullptr) throw std::invalid_argument("unexpected nullptr");
+    return reinterpret_cast<Index*>(p);
+}
+const Index* as_index(const nsp_index_t* p) {
+    if (p == nullptr) throw std::invalid_argument("unexpected nullptr");
+    return reinterpret_cast<const Index*>(p);
+}
+IDSelector* as_sel(nsp_id_selector_t* p) { return reinterpret_cast<IDSelector*>(p); }
+SearchParameters* as_params(const nsp_search_params_t* p) {
+    return reinterpret_cast<SearchParameters*>(const_cast<nsp_search_params_t*>(p));
+}
+template <class T>
+void check_out(T** out) {
+    if (out == nullptr) throw std::invalid_argument("unexpected nullptr");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* nsp_last_error(void) { return g_error.c_str(); }
+
+nsp_status_t nsp_index_factory(int dim, const char* description, nsp_index_t** out) {
+    return guarded([&] {
+        check_out(out);
+        *out = reinterpret_cast<nsp_index_t*>(index_factory(dim, description));
+    });
+}
+
+nsp_status_t nsp_index_free(nsp_index_t* index) {
+    return guarded([&] { delete reinterpret_cast<Index*>(index); });
+}
+
+nsp_status_t nsp_index_add(nsp_index_t* index, int32_t n, const int32_t* indptr,
+                           const uint16_t* indices, const float* values) {
+    return guarded([&] { as_index(index)->add(n, indptr, indices, values); });
+}
+
+nsp_status_t nsp_index_add_with_ids(nsp_index_t* index, int32_t n, const int32_t* indptr,
+                                    const uint16_t* indices, const float* values,
+                                    const int32_t* ids) {
+    return guarded([&] { as_index(index)->add_with_ids(n, indptr, indices, values, ids); });
+}
+
+nsp_status_t nsp_index_build(nsp_index_t* index) {
+    return guarded([&] { as_index(index)->build(); });
+}
+
+nsp_status_t nsp_index_search(nsp_index_t* index, int32_t n, const int32_t* indptr,
+                              const uint16_t* indices, const float* values, int k,
+                              float* distances, int32_t* labels,
+                              const nsp_search_params_t* params) {
+    return guarded([&] {
+        as_index(index)->search(n, indptr, indices, values, k, distances, labels,
+                                as_params(params));
+    });
+}
+
+nsp_status_t nsp_index_num_vectors(const nsp_index_t* index, int64_t* out) {
+    return guarded([&] {
+        check_out(&out);
+        *out = static_cast<int64_t>(as_index(index)->num_vectors());
+    });
+}
+
+nsp_status_t nsp_index_dimension(const nsp_index_t* index, int32_t* out) {
+    return guarded([&] {
+        check_out(&out);
+        *out = as_index(index)->get_dimension();
+    });
+}
+
+nsp_status_t nsp_index_fourcc(const nsp_index_t* index, char out[4]) {
+    return guarded([&] {
+        if (out == nullptr) throw std::invalid_argument("unexpected nullptr");
+        const auto id = as_index(index)->id();
+        std::memcpy(out, id.data(), 4);
+    });
+}
+
+nsp_status_t nsp_index_read_csr(nsp_index_t* index, const char* path, int residency) {
+    return guarded([&] {
+        as_index(index)->read_csr(path, residency == 1 ? Residency::kMmap : Residency::kInMemory);
+    });
+}
+
+nsp_status_t nsp_write_index(nsp_index_t* index, const char* path) {
+    return guarded([&] { write_index(as_index(index), path); });
+}
+
+nsp_status_t nsp_read_index(const char* path, int io_flags, nsp_index_t** out) {
+    return guarded([&] {
+        check_out(out);
+        *out = reinterpret_cast<nsp_index_t*>(read_index(path, io_flags));
+    });
+}
+
+nsp_status_t nsp_id_selector_set_new(size_t n, const int32_t* ids, nsp_id_selector_t** out) {
+    return guarded([&] {
+        check_out(out);
+        if (n > 0 && ids == nullptr) throw std::invalid_argument("unexpected nullptr");
+        *out = reinterpret_cast<nsp_id_selector_t*>(new SetIDSelector(n, ids));
+    });
+}
+
+nsp_status_t nsp_id_selector_array_new(size_t n, const int32_t* ids, nsp_id_selector_t** out) {
+    return guarded([&] {
+        check_out(out);
+        if (n > 0 && ids == nullptr) throw std::invalid_argument("unexpected nullptr");
+        *out = reinterpret_cast<nsp_id_selector_t*>(new ArrayIDSelector(n, ids));
+    });
+}
+
+nsp_status_t nsp_id_selector_not_new(nsp_id_selector_t* inner, nsp_id_selector_t** out) {
+    return guarded([&] {
+        check_out(out);
+        if (inner == nullptr) throw std::invalid_argument("unexpected nullptr");
+        *out = reinterpret_cast<nsp_id_selector_t*>(new NotIDSelector(as_sel(inner)));
+    });
+}
+
+nsp_status_t nsp_id_selector_bitmap_new(int64_t n_bits, const uint64_t* bits,
+                                        nsp_id_selector_t** out) {
+    return guarded([&] {
+        check_out(out);
+        *out = reinterpret_cast<nsp_id_selector_t*>(new BitmapIDSelector(n_bits, bits));
+    });
+}
+
+nsp_status_t nsp_id_selector_is_member(const nsp_id_selector_t* sel, int32_t id, int* out) {
+    return guarded([&] {
+        if (sel == nullptr || out == nullptr) throw std::invalid_argument("unexpected nullptr");
+        *out = reinterpret_cast<const IDSelector*>(sel)->is_member(id) ? 1 : 0;
+    });
+}
+
+nsp_status_t nsp_id_selector_free(nsp_id_selector_t* sel) {
+    return guarded([&] { delete as_sel(sel); });
+}
+
+nsp_status_t nsp_search_params_new(nsp_search_params_t** out) {
+    return guarded([&] {
+        check_out(out);
+        *out = reinterpret_cast<nsp_search_params_t*>(new SearchParameters());
+    });
+}
+
+nsp_status_t nsp_seismic_search_params_new(int cut, float heap_factor,
+                                           nsp_search_params_t** out) {
+    return guarded([&] {
+        check_out(out);
+        *out = reinterpret_cast<nsp_search_params_t*>(new SeismicSearchParameters(cut, heap_factor));
+    });
+}
+
+nsp_status_t nsp_seismic_sq_search_params_new(float vmin, float vmax, int cut,
+                                              float heap_factor, nsp_search_params_t** out) {
+    return guarded([&] {
+        check_out(out);
+        *out = reinterpret_cast<nsp_search_params_t*>(
+            new SeismicSQSearchParameters(vmin, vmax, cut, heap_factor));
+    });
+}
+
+nsp_status_t nsp_search_params_set_id_selector(nsp_search_params_t* params,
+                                               nsp_id_selector_t* sel) {
+    return guarded([&] {
+        if (params == nullptr) throw std::invalid_argument("unexpected nullptr");
+        as_params(params)->set_id_selector(as_sel(sel));
+    });
+}
+
+nsp_status_t nsp_search_params_set_engine(nsp_search_params_t* params, int plain,
+                                          int warps_per_block) {
+    return guarded([&] {
+        if (params == nullptr) throw std::invalid_argument("unexpected nullptr");
+        if (warps_per_block < 0 || warps_per_block > 8)
+            throw std::invalid_argument("warps_per_block must be in [0, 8]");
+        as_params(params)->engine.plain = plain != 0;
+        as_params(params)->engine.warps_per_block = warps_per_block;
+    });
+}
+
+nsp_status_t nsp_search_params_free(nsp_search_params_t* params) {
+    return guarded([&] { delete as_params(params); });
+}
+
+nsp_status_t nsp_last_search_stats(nsp_search_stats_t* out) {
+    return guarded([&] {
+        if (out == nullptr) throw std::invalid_argument("unexpected nullptr");
+        const SearchStats& s = last_search_stats();
+        out->docs_scored = s.docs_scored;
+        out->blocks_visited = s.blocks_visited;
+        out->bytes = s.bytes;
+        out->lists_probed = s.lists_probed;
+        out->kernel_ms = s.kernel_ms;
+        out->launches = s.launches;
+    });
+}
+
+nsp_status_t nsp_index_search_device(nsp_index_t* index, int32_t n, const int32_t* d_indptr,
+                                     const uint16_t* d_indices, const float* d_values,
+                                     int32_t max_row_nnz, int k, float* d_distances,
+                                     int32_t* d_labels, const nsp_search_params_t* params,
+                                     void* cuda_stream) {
+    return guarded([&] {
+        detail::search_device(as_index(index), n, d_indptr, d_indices, d_values, max_row_nnz, k,
+                              d_distances, d_labels, as_params(params),
+                              static_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
+nsp_status_t nsp_device_info(int32_t* n_devices, char* name, size_t name_len) {
+    return guarded([&] {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
+        if (n_devices != nullptr) *n_devices = n;
+        if (name != nullptr && name_len > 0) {
+            name[0] = '\0';
+            if (n > 0) {
+                int dev = 0;
+                cudaGetDevice(&dev);
+                cudaDeviceProp prop{};
+                if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess) {
+                    std::strncpy(name, prop.name, name_len - 1);
+                    name[name_len - 1] = '\0';
+                }
+            }
+        }
+    });
+}
+
+}  // extern "C"

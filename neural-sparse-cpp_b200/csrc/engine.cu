@@ -1,0 +1,684 @@
+// Host-side engine: device buffers, workspaces, index uploads and the search
+// drivers. See engine.h.
+#include "engine.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <utility>
+
+#include "scan.h"
+
+namespace nsp {
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        throw std::runtime_error(std::string("CUDA error in ") + what + ": " +
+                                 cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+    }
+}
+
+int device_sm_count() {
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    int sms = 0;
+    cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev),
+               "cudaDeviceGetAttribute");
+    return sms;
+}
+
+static int max_smem_optin() {
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    int v = 0;
+    cuda_check(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev),
+               "cudaDeviceGetAttribute");
+    return v;
+}
+
+// ------------------------------------------------------------ workspace --
+
+Workspace::Workspace() {
+    cuda_check(cudaGetDevice(&device_), "cudaGetDevice");
+    cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+}
+
+Workspace::~Workspace() {
+    // Runs at thread exit; the CUDA context may already be gone at process
+    // exit, so failures here are ignored.
+    for (int i = 0; i < kNumSlots; ++i) {
+        if (dptr_[i] != nullptr) cudaFree(dptr_[i]);
+        if (hptr_[i] != nullptr) cudaFreeHost(hptr_[i]);
+    }
+    if (stream_ != nullptr) cudaStreamDestroy(stream_);
+}
+
+Workspace& Workspace::get() {
+    thread_local std::unique_ptr<Workspace> ws;
+    if (!ws) ws.reset(new Workspace());
+    return *ws;
+}
+
+void* Workspace::dev(Slot s, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (dcap_[s] < bytes) {
+        cuda_check(cudaStreamSynchronize(stream_), "workspace sync");
+        if (dptr_[s] != nullptr) cudaFree(dptr_[s]);
+        dptr_[s] = nullptr;
+        const size_t cap = bytes + bytes / 2;
+        cuda_check(cudaMalloc(&dptr_[s], cap), "workspace cudaMalloc");
+        dcap_[s] = cap;
+    }
+    return dptr_[s];
+}
+
+void* Workspace::pinned(Slot s, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (hcap_[s] < bytes) {
+        cuda_check(cudaStreamSynchronize(stream_), "workspace sync");
+        if (hptr_[s] != nullptr) cudaFreeHost(hptr_[s]);
+        hptr_[s] = nullptr;
+        const size_t cap = bytes + bytes / 2;
+        cuda_check(cudaHostAlloc(&hptr_[s], cap, cudaHostAllocDefault), "cudaHostAlloc");
+        hcap_[s] = cap;
+    }
+    return hptr_[s];
+}
+
+// ------------------------------------------------------------- host CSR --
+
+void HostCsr::append(int32_t n, const int32_t* ip, const uint16_t* idx, const uint8_t* vals) {
+    if (n <= 0) return;
+    const int64_t add = static_cast<int64_t>(ip[n]) - ip[0];
+    const int64_t base = nnz();
+    if (base + add > INT32_MAX) throw std::invalid_argument("too many non-zeros for int32 offsets");
+    indices.insert(indices.end(), idx + ip[0], idx + ip[0] + add);
+    values.insert(values.end(), vals + static_cast<size_t>(ip[0]) * esz,
+                  vals + static_cast<size_t>(ip[0] + add) * esz);
+    indptr.reserve(indptr.size() + n);
+    for (int32_t i = 1; i <= n; ++i)
+        indptr.push_back(static_cast<int32_t>(base + (ip[i] - ip[0])));
+}
+
+// -------------------------------------------------------- forward index --
+
+namespace {
+
+__global__ void row_units_kernel(const int32_t* indptr, int32_t n, int64_t* units) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t len = indptr[i + 1] - indptr[i];
+        units[i] = (len + kRowAlign - 1) / kRowAlign;
+    }
+}
+
+// One warp per row: copy ids and value bytes to the padded position, zero
+// the padding.
+__global__ void pad_rows_kernel(const int32_t* indptr, const uint16_t* idx, const uint8_t* val,
+                                int32_t n, int esz, const int64_t* off16, uint2* rowinfo,
+                                uint16_t* pidx, uint8_t* pval) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t r = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5; r < n;
+         r += warps) {
+        const int64_t s = indptr[r];
+        const int64_t len = indptr[r + 1] - s;
+        const int64_t dst = off16[r] * kRowAlign;
+        const int64_t plen = ((len + kRowAlign - 1) / kRowAlign) * kRowAlign;
+        for (int64_t j = lane; j < plen; j += 32) {
+            pidx[dst + j] = j < len ? idx[s + j] : static_cast<uint16_t>(0);
+        }
+        for (int64_t j = lane; j < plen * esz; j += 32) {
+            pval[dst * esz + j] = j < len * esz ? val[s * esz + j] : static_cast<uint8_t>(0);
+        }
+        if (lane == 0) rowinfo[r] = make_uint2(static_cast<uint32_t>(off16[r]),
+                                               static_cast<uint32_t>(len));
+    }
+}
+
+}  // namespace
+
+void ForwardDevice::upload(const HostCsr& h) {
+    cudaStream_t s = Workspace::get().stream();
+    n_docs_ = static_cast<int32_t>(h.n());
+    dim_ = h.dim;
+    esz_ = h.esz;
+    if (n_docs_ == 0) {
+        rowinfo_.reset();
+        idx_.reset();
+        val_.reset();
+        return;
+    }
+    const int64_t nnz = h.nnz();
+    DevArray<int32_t> d_indptr;
+    DevArray<uint16_t> d_idx;
+    DevArray<uint8_t> d_val;
+    d_indptr.upload(h.indptr.data(), h.indptr.size(), s);
+    d_idx.upload(h.indices.data(), static_cast<size_t>(nnz), s);
+    d_val.upload(h.values.data(), static_cast<size_t>(nnz) * esz_, s);
+    DevArray<int64_t> units(static_cast<size_t>(n_docs_) + 1);
+    row_units_kernel<<<std::min<int64_t>((n_docs_ + 255) / 256, 148 * 16), 256, 0, s>>>(
+        d_indptr.data(), n_docs_, units.data());
+    cuda_check(cudaGetLastError(), "row_units_kernel");
+    // exclusive scan in place over n+1 entries (last entry = total units)
+    cuda_check(cudaMemsetAsync(units.data() + n_docs_, 0, sizeof(int64_t), s), "memset");
+    exclusive_scan_i64(units.data(), units.data(), static_cast<int64_t>(n_docs_) + 1, s);
+    int64_t total_units = 0;
+    cuda_check(cudaMemcpyAsync(&total_units, units.data() + n_docs_, sizeof(int64_t),
+                               cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    if (total_units > static_cast<int64_t>(UINT32_MAX))
+        throw std::invalid_argument("forward index too large for 32-bit row offsets");
+    const size_t padded = static_cast<size_t>(total_units) * kRowAlign;
+    rowinfo_.resize(static_cast<size_t>(n_docs_));
+    idx_.resize(std::max<size_t>(padded, 16));
+    val_.resize(std::max<size_t>(padded * esz_, 16));
+    pad_rows_kernel<<<148 * 16, 256, 0, s>>>(d_indptr.data(), d_idx.data(), d_val.data(), n_docs_,
+                                             esz_, units.data(), rowinfo_.data(), idx_.data(),
+                                             val_.data());
+    cuda_check(cudaGetLastError(), "pad_rows_kernel");
+    cuda_check(cudaStreamSynchronize(s), "sync");
+}
+
+FwdView ForwardDevice::view() const {
+    FwdView v;
+    v.n_docs = n_docs_;
+    v.dim = dim_;
+    v.rowinfo = rowinfo_.data();
+    v.idx = idx_.data();
+    v.val = val_.data();
+    return v;
+}
+
+size_t ForwardDevice::device_bytes() const {
+    return rowinfo_.size() * sizeof(uint2) + idx_.size() * 2 + val_.size();
+}
+
+// --------------------------------------------------------- SEISMIC lists --
+
+namespace {
+
+// One CTA per list: the list's summary-term bitmap and per-word prefix.
+__global__ void list_meta_kernel(const int64_t* ltp, const uint16_t* sterm, int32_t n_lists,
+                                 int words, uint2* lmeta) {
+    extern __shared__ uint32_t bits[];
+    __shared__ int warp_sums[32];
+    for (int32_t t = blockIdx.x; t < n_lists; t += gridDim.x) {
+        for (int w = threadIdx.x; w < words; w += blockDim.x) bits[w] = 0u;
+        __syncthreads();
+        for (int64_t c = ltp[t] + threadIdx.x; c < ltp[t + 1]; c += blockDim.x) {
+            const uint32_t term = sterm[c];
+            atomicOr(&bits[term >> 5], 1u << (term & 31));
+        }
+        __syncthreads();
+        // exclusive scan of popcounts over `words` entries, chunked per thread
+        const int per = (words + blockDim.x - 1) / blockDim.x;
+        const int w0 = threadIdx.x * per;
+        const int w1 = min(words, w0 + per);
+        int local = 0;
+        for (int w = w0; w < w1; ++w) local += __popc(bits[w]);
+        const int lane = threadIdx.x & 31;
+        const int wid = threadIdx.x >> 5;
+        int incl = local;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) warp_sums[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            const int nw = blockDim.x >> 5;
+            int v = lane < nw ? warp_sums[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += y;
+            }
+            if (lane < nw) warp_sums[lane] = v;  // inclusive
+        }
+        __syncthreads();
+        int run = incl - local + (wid > 0 ? warp_sums[wid - 1] : 0);
+        uint2* row = lmeta + static_cast<size_t>(t) * words;
+        for (int w = w0; w < w1; ++w) {
+            row[w] = make_uint2(bits[w], static_cast<uint32_t>(run));
+            run += __popc(bits[w]);
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+void SeismicDevice::upload(const SeismicHost& h, int dim) {
+    cudaStream_t s = Workspace::get().stream();
+    n_lists_ = h.n_lists();
+    words_ = (dim + 31) / 32;
+    max_blocks_ = 0;
+    for (int32_t t = 0; t < n_lists_; ++t)
+        max_blocks_ = std::max<int32_t>(max_blocks_, static_cast<int32_t>(h.lbp[t + 1] - h.lbp[t]));
+    lbp_.upload(h.lbp.data(), h.lbp.size(), s);
+    bdp_.upload(h.bdp.data(), h.bdp.size(), s);
+    docs_.upload(h.docs.data(), h.docs.size(), s);
+    ltp_.upload(h.ltp.data(), h.ltp.size(), s);
+    srun_.upload(h.srun.data(), h.srun.size(), s);
+    esz_ = h.esz;
+    sterm_.upload(h.sterm.data(), h.sterm.size(), s);
+    sblk_.upload(h.sblk.data(), h.sblk.size(), s);
+    sval_.upload(h.sval.data(), h.sval.size(), s);
+    if (n_lists_ > 0) {
+        lmeta_.resize(static_cast<size_t>(n_lists_) * words_);
+        list_meta_kernel<<<std::min(n_lists_, 148 * 8), 256, static_cast<size_t>(words_) * 4, s>>>(
+            ltp_.data(), sterm_.data(), n_lists_, words_, lmeta_.data());
+        cuda_check(cudaGetLastError(), "list_meta_kernel");
+    }
+    cuda_check(cudaStreamSynchronize(s), "sync");
+}
+
+void SeismicDevice::download(SeismicHost& h) const {
+    cudaStream_t s = Workspace::get().stream();
+    h.esz = esz_;
+    auto get64 = [&](const DevArray<int64_t>& d, std::vector<int64_t>& v, size_t n) {
+        v.resize(n);
+        d.download(v.data(), n, s);
+    };
+    const size_t nl = static_cast<size_t>(n_lists_) + 1;
+    get64(lbp_, h.lbp, nl);
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    const size_t nb = static_cast<size_t>(h.lbp.back()) + 1;
+    get64(bdp_, h.bdp, nb);
+    get64(ltp_, h.ltp, nl);
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    const size_t nd = static_cast<size_t>(h.bdp.back());
+    const size_t nc = static_cast<size_t>(h.ltp.back());
+    h.docs.resize(nd);
+    docs_.download(h.docs.data(), nd, s);
+    h.sterm.resize(nc);
+    sterm_.download(h.sterm.data(), nc, s);
+    get64(srun_, h.srun, nc + 1);
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    const size_t ne = static_cast<size_t>(h.srun.back());
+    h.sblk.resize(ne);
+    sblk_.download(h.sblk.data(), ne, s);
+    h.sval.resize(ne * static_cast<size_t>(esz_));
+    sval_.download(h.sval.data(), ne * static_cast<size_t>(esz_), s);
+    cuda_check(cudaStreamSynchronize(s), "sync");
+}
+
+SeismicView SeismicDevice::view() const {
+    SeismicView v;
+    v.n_lists = n_lists_;
+    v.words = words_;
+    v.max_blocks = std::max(max_blocks_, 1);
+    v.lbp = lbp_.data();
+    v.bdp = bdp_.data();
+    v.docs = docs_.data();
+    v.lmeta = lmeta_.data();
+    v.ltp = ltp_.data();
+    v.srun = srun_.data();
+    v.sblk = sblk_.data();
+    v.sval = sval_.data();
+    return v;
+}
+
+size_t SeismicDevice::device_bytes() const {
+    return (lbp_.size() + bdp_.size() + ltp_.size() + srun_.size()) * 8 + docs_.size() * 4 +
+           lmeta_.size() * 8 + sblk_.size() * 2 + sterm_.size() * 2 + sval_.size();
+}
+
+// -------------------------------------------------------------- queries --
+
+QueryBatch canonicalize(int32_t n, const int32_t* indptr, const uint16_t* idx, const float* val,
+                        int dim) {
+    QueryBatch q;
+    q.n = n;
+    bool canonical = indptr[0] == 0;
+    int32_t max_nnz = 0;
+    for (int32_t i = 0; i < n; ++i) {
+        const int32_t s = indptr[i], e = indptr[i + 1];
+        if (e < s) throw std::invalid_argument("query indptr is not monotonic");
+        max_nnz = std::max(max_nnz, e - s);
+        for (int32_t j = s; j < e; ++j) {
+            if (idx[j] >= dim) throw std::invalid_argument("query term out of range");
+            if (j > s && idx[j] <= idx[j - 1]) canonical = false;
+        }
+    }
+    q.max_nnz = max_nnz;
+    if (canonical) {
+        q.ip = indptr;
+        q.ix = idx;
+        q.vv = val;
+        return q;
+    }
+    q.indptr.assign(1, 0);
+    q.indptr.reserve(n + 1);
+    std::vector<std::pair<uint16_t, int32_t>> row;
+    max_nnz = 0;
+    for (int32_t i = 0; i < n; ++i) {
+        const int32_t s = indptr[i], e = indptr[i + 1];
+        row.clear();
+        for (int32_t j = s; j < e; ++j) row.emplace_back(idx[j], j);
+        std::sort(row.begin(), row.end());
+        int32_t kept = 0;
+        for (size_t r = 0; r < row.size(); ++r) {
+            // keep the last occurrence of a repeated term
+            if (r + 1 < row.size() && row[r + 1].first == row[r].first) continue;
+            q.idx.push_back(row[r].first);
+            q.val.push_back(val[row[r].second]);
+            ++kept;
+        }
+        max_nnz = std::max(max_nnz, kept);
+        q.indptr.push_back(static_cast<int32_t>(q.idx.size()));
+    }
+    q.max_nnz = max_nnz;
+    q.ip = q.indptr.data();
+    q.ix = q.idx.data();
+    q.vv = q.val.data();
+    return q;
+}
+
+// ----------------------------------------------------------- search ------
+
+namespace {
+
+struct Uploaded {
+    int32_t* indptr;
+    uint16_t* idx;
+    float* val;
+    int64_t nnz;
+};
+
+Uploaded upload_queries(Workspace& ws, const QueryBatch& q) {
+    cudaStream_t s = ws.stream();
+    const int64_t nnz = q.ip[q.n] - q.ip[0];
+    Uploaded u;
+    u.nnz = nnz;
+    auto* hi = static_cast<int32_t*>(ws.pinned(Workspace::kQIndptr, (q.n + 1) * sizeof(int32_t)));
+    auto* hx = static_cast<uint16_t*>(ws.pinned(Workspace::kQIdx, nnz * sizeof(uint16_t)));
+    auto* hv = static_cast<float*>(ws.pinned(Workspace::kQVal, nnz * sizeof(float)));
+    const int32_t base = q.ip[0];
+    for (int32_t i = 0; i <= q.n; ++i) hi[i] = q.ip[i] - base;
+    std::memcpy(hx, q.ix + base, nnz * sizeof(uint16_t));
+    std::memcpy(hv, q.vv + base, nnz * sizeof(float));
+    u.indptr = static_cast<int32_t*>(ws.dev(Workspace::kQIndptr, (q.n + 1) * sizeof(int32_t)));
+    u.idx = static_cast<uint16_t*>(ws.dev(Workspace::kQIdx, nnz * sizeof(uint16_t) + 16));
+    u.val = static_cast<float*>(ws.dev(Workspace::kQVal, nnz * sizeof(float) + 16));
+    cuda_check(cudaMemcpyAsync(u.indptr, hi, (q.n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s),
+               "H2D queries");
+    cuda_check(cudaMemcpyAsync(u.idx, hx, nnz * sizeof(uint16_t), cudaMemcpyHostToDevice, s),
+               "H2D queries");
+    cuda_check(cudaMemcpyAsync(u.val, hv, nnz * sizeof(float), cudaMemcpyHostToDevice, s),
+               "H2D queries");
+    return u;
+}
+
+const uint64_t* upload_sel(Workspace& ws, const std::vector<uint64_t>* sel) {
+    if (sel == nullptr) return nullptr;
+    const size_t bytes = sel->size() * sizeof(uint64_t);
+    auto* h = static_cast<uint64_t*>(ws.pinned(Workspace::kSel, bytes));
+    std::memcpy(h, sel->data(), bytes);
+    auto* d = static_cast<uint64_t*>(ws.dev(Workspace::kSel, bytes));
+    cuda_check(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, ws.stream()), "H2D selector");
+    return d;
+}
+
+void download_results(Workspace& ws, int32_t n, int k, const float* dd, const int32_t* dl,
+                      float* out_d, int32_t* out_l) {
+    cudaStream_t s = ws.stream();
+    const size_t cnt = static_cast<size_t>(n) * k;
+    auto* hd = static_cast<float*>(ws.pinned(Workspace::kOutD, cnt * sizeof(float)));
+    auto* hl = static_cast<int32_t*>(ws.pinned(Workspace::kOutL, cnt * sizeof(int32_t)));
+    cuda_check(cudaMemcpyAsync(hd, dd, cnt * sizeof(float), cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaMemcpyAsync(hl, dl, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaStreamSynchronize(s), "search sync");
+    std::memcpy(out_d, hd, cnt * sizeof(float));
+    std::memcpy(out_l, hl, cnt * sizeof(int32_t));
+}
+
+int val_kind_of(int qbits) { return qbits == 0 ? kF32 : (qbits == 8 ? kU8 : kU16); }
+
+struct SeismicPlan {
+    int wpb;
+    int blocks;
+    size_t smem_per_warp;
+};
+
+SeismicPlan plan_seismic(int kind, int words, int qcap, int k, int n_queries, int wpb_req) {
+    SeismicPlan p;
+    p.smem_per_warp = seismic_smem_per_warp(kind, words, qcap, k);
+    const size_t limit = static_cast<size_t>(max_smem_optin());
+    if (p.smem_per_warp > limit)
+        throw std::invalid_argument("query too long or k too large for the device search kernel");
+    int wpb = wpb_req > 0 ? wpb_req : 4;
+    while (wpb > 1 && p.smem_per_warp * wpb > limit) wpb >>= 1;
+    p.wpb = wpb;
+    int per_sm = seismic_max_blocks_per_sm(kind, wpb, p.smem_per_warp * wpb);
+    if (per_sm < 1) per_sm = 1;
+    const int want = (n_queries + wpb - 1) / wpb;
+    p.blocks = std::max(1, std::min(want, device_sm_count() * per_sm));
+    return p;
+}
+
+void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
+                 const int32_t* d_indptr, const uint16_t* d_idx, const void* d_vals, int32_t qcap,
+                 const SeismicSearchArgs& args, const uint64_t* d_sel, float* d_out,
+                 int32_t* d_lab, cudaStream_t s, Workspace& ws, SearchStats* stats) {
+    const int kind = val_kind_of(args.qbits);
+    SeismicLaunch a{};
+    a.fwd = fwd.view();
+    a.ix = ix.view();
+    a.q.n = n;
+    a.q.indptr = d_indptr;
+    a.q.idx = d_idx;
+    a.q.val = d_vals;
+    a.k = args.k;
+    a.cut = args.cut;
+    a.heap_factor = args.heap_factor;
+    a.decode_scale = args.decode_scale;
+    a.sel_bits = d_sel;
+    a.out_d = d_out;
+    a.out_l = d_lab;
+    a.qcap = std::max(qcap, 1);
+    auto* st = static_cast<unsigned long long*>(
+        ws.dev(Workspace::kStats, kStatCount * sizeof(unsigned long long)));
+    cuda_check(cudaMemsetAsync(st, 0, kStatCount * sizeof(unsigned long long), s), "memset");
+    a.stats = st;
+    cudaEvent_t e0, e1;
+    cuda_check(cudaEventCreate(&e0), "event");
+    cuda_check(cudaEventCreate(&e1), "event");
+    int launches = 0;
+    if (!args.plain) {
+        const SeismicPlan p = plan_seismic(kind, a.ix.words, a.qcap, a.k, n, args.warps_per_block);
+        const size_t warps = static_cast<size_t>(p.blocks) * p.wpb;
+        a.bscore = static_cast<float*>(
+            ws.dev(Workspace::kBScore, warps * a.ix.max_blocks * sizeof(float)));
+        a.work_counter = static_cast<int32_t*>(ws.dev(Workspace::kCounter, sizeof(int32_t)));
+        cuda_check(cudaMemsetAsync(a.work_counter, 0, sizeof(int32_t), s), "memset");
+        a.first_query = 0;
+        cuda_check(cudaEventRecord(e0, s), "event");
+        cuda_check(launch_seismic(kind, a, p.wpb, p.blocks, s), "seismic search launch");
+        cuda_check(cudaEventRecord(e1, s), "event");
+        launches = 1;
+    } else {
+        // One launch per query: a single warp walks the query (the per-query
+        // path the batched launch is measured against).
+        a.bscore = static_cast<float*>(ws.dev(Workspace::kBScore, a.ix.max_blocks * sizeof(float)));
+        a.work_counter = nullptr;
+        cuda_check(cudaEventRecord(e0, s), "event");
+        for (int32_t q = 0; q < n; ++q) {
+            a.first_query = q;
+            a.q.n = q + 1;
+            cuda_check(launch_seismic(kind, a, 1, 1, s), "seismic search launch");
+        }
+        cuda_check(cudaEventRecord(e1, s), "event");
+        launches = n;
+    }
+    if (stats != nullptr) {
+        unsigned long long h[kStatCount];
+        cuda_check(cudaMemcpyAsync(h, st, sizeof(h), cudaMemcpyDeviceToHost, s), "D2H stats");
+        cuda_check(cudaStreamSynchronize(s), "sync");
+        float ms = 0.0f;
+        cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event time");
+        stats->docs_scored = h[kStatDocsScored];
+        stats->blocks_visited = h[kStatBlocksVisited];
+        stats->bytes = h[kStatBytes];
+        stats->lists_probed = h[kStatListsProbed];
+        stats->kernel_ms = ms;
+        stats->launches = launches;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+}
+
+}  // namespace
+
+void seismic_search(const ForwardDevice& fwd, const SeismicDevice& ix, const QueryBatch& q,
+                    const SeismicSearchArgs& args, const std::vector<uint64_t>* sel_bits,
+                    float* out_d, int32_t* out_l, SearchStats* stats) {
+    Workspace& ws = Workspace::get();
+    cudaStream_t s = ws.stream();
+    const Uploaded u = upload_queries(ws, q);
+    const void* vals = u.val;
+    if (args.qbits != 0) {
+        void* codes = ws.dev(Workspace::kQCode, static_cast<size_t>(u.nnz) * 2 + 16);
+        cuda_check(launch_sq_encode(u.val, codes, u.nnz, args.qbits, args.q_vmin, args.q_scale, s),
+                   "query encode");
+        vals = codes;
+    }
+    const uint64_t* d_sel = upload_sel(ws, sel_bits);
+    const size_t cnt = static_cast<size_t>(q.n) * args.k;
+    auto* dd = static_cast<float*>(ws.dev(Workspace::kOutD, cnt * sizeof(float)));
+    auto* dl = static_cast<int32_t*>(ws.dev(Workspace::kOutL, cnt * sizeof(int32_t)));
+    run_seismic(fwd, ix, q.n, u.indptr, u.idx, vals, q.max_nnz, args, d_sel, dd, dl, s, ws, stats);
+    download_results(ws, q.n, args.k, dd, dl, out_d, out_l);
+}
+
+void seismic_search_device(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
+                           const int32_t* d_indptr, const uint16_t* d_idx, const void* d_val,
+                           int32_t max_nnz, const SeismicSearchArgs& args, const uint64_t* d_sel,
+                           float* d_out, int32_t* d_lab, cudaStream_t s, SearchStats* stats) {
+    Workspace& ws = Workspace::get();
+    run_seismic(fwd, ix, n, d_indptr, d_idx, d_val, max_nnz, args, d_sel, d_out, d_lab, s, ws,
+                stats);
+}
+
+void exact_search(const ForwardDevice& fwd, const QueryBatch& q, int k, int mode,
+                  const std::vector<uint64_t>* sel_bits, float* out_d, int32_t* out_l,
+                  SearchStats* stats) {
+    Workspace& ws = Workspace::get();
+    cudaStream_t s = ws.stream();
+    const Uploaded u = upload_queries(ws, q);
+    const uint64_t* d_sel = upload_sel(ws, sel_bits);
+    const size_t cnt = static_cast<size_t>(q.n) * k;
+    auto* dd = static_cast<float*>(ws.dev(Workspace::kOutD, cnt * sizeof(float)));
+    auto* dl = static_cast<int32_t*>(ws.dev(Workspace::kOutL, cnt * sizeof(int32_t)));
+
+    ExactLaunch a{};
+    a.fwd = fwd.view();
+    a.q.n = q.n;
+    a.q.indptr = u.indptr;
+    a.q.idx = u.idx;
+    a.q.val = u.val;
+    a.k = k;
+    a.mode = mode;
+    a.sel_bits = d_sel;
+    a.qcap = std::max(q.max_nnz, 1);
+    a.out_d = dd;
+    a.out_l = dl;
+    const int words = (fwd.view().dim + 31) / 32;
+    const size_t limit = static_cast<size_t>(max_smem_optin());
+    const bool values_global = exact_smem(words, a.qcap) > limit;
+    if (exact_smem(words, 0) > limit)
+        throw std::invalid_argument("vocabulary too large for the exact search kernel");
+    const int groups = (q.n + 31) / 32;
+    const int sms = device_sm_count();
+    int tiles = std::max(1, (2 * sms + groups - 1) / groups);
+    const int32_t nd = std::max(fwd.n_docs(), 1);
+    tiles = std::min(tiles, std::max(1, nd / 64));
+    a.docs_per_tile = (nd + tiles - 1) / tiles;
+    tiles = (nd + a.docs_per_tile - 1) / a.docs_per_tile;
+    const size_t lanes = static_cast<size_t>(groups) * tiles * 8 * 32;
+    a.heap_d = static_cast<float*>(ws.dev(Workspace::kHeapD, lanes * k * sizeof(float)));
+    a.heap_l = static_cast<int32_t*>(ws.dev(Workspace::kHeapL, lanes * k * sizeof(int32_t)));
+    const size_t cands = static_cast<size_t>(groups) * 32 * tiles * k;
+    a.cand_d = static_cast<float*>(ws.dev(Workspace::kCandD, cands * sizeof(float)));
+    a.cand_l = static_cast<int32_t*>(ws.dev(Workspace::kCandL, cands * sizeof(int32_t)));
+    a.qval_global = values_global
+                        ? static_cast<float*>(ws.dev(Workspace::kQValG,
+                                                     static_cast<size_t>(groups) * tiles * 32 *
+                                                         a.qcap * sizeof(float)))
+                        : nullptr;
+    auto* st = static_cast<unsigned long long*>(
+        ws.dev(Workspace::kStats, kStatCount * sizeof(unsigned long long)));
+    cuda_check(cudaMemsetAsync(st, 0, kStatCount * sizeof(unsigned long long), s), "memset");
+    a.stats = st;
+    cudaEvent_t e0, e1;
+    cuda_check(cudaEventCreate(&e0), "event");
+    cuda_check(cudaEventCreate(&e1), "event");
+    cuda_check(cudaEventRecord(e0, s), "event");
+    if (fwd.n_docs() > 0) {
+        cuda_check(launch_exact(a, tiles, s), "exact search launch");
+    } else {
+        cuda_check(cudaMemsetAsync(dd, 0, cnt * sizeof(float), s), "memset");
+    }
+    cuda_check(cudaEventRecord(e1, s), "event");
+    if (fwd.n_docs() == 0) {
+        // nothing indexed: every slot is padding
+        cuda_check(cudaStreamSynchronize(s), "sync");
+        for (size_t i = 0; i < cnt; ++i) {
+            out_d[i] = -1.0f;
+            out_l[i] = -1;
+        }
+    } else {
+        download_results(ws, q.n, k, dd, dl, out_d, out_l);
+    }
+    if (stats != nullptr) {
+        unsigned long long h[kStatCount];
+        cuda_check(cudaMemcpyAsync(h, st, sizeof(h), cudaMemcpyDeviceToHost, s), "D2H stats");
+        cuda_check(cudaStreamSynchronize(s), "sync");
+        float ms = 0.0f;
+        cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event time");
+        stats->bytes = h[kStatBytes];
+        stats->kernel_ms = ms;
+        stats->launches = 2;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+}
+
+void exact_list_search(const ForwardDevice& fwd, const QueryBatch& q, const SeismicSearchArgs& args,
+                       const std::vector<int32_t>& ids, float* out_d, int32_t* out_l) {
+    Workspace& ws = Workspace::get();
+    cudaStream_t s = ws.stream();
+    const Uploaded u = upload_queries(ws, q);
+    const void* vals = u.val;
+    if (args.qbits != 0) {
+        void* codes = ws.dev(Workspace::kQCode, static_cast<size_t>(u.nnz) * 2 + 16);
+        cuda_check(launch_sq_encode(u.val, codes, u.nnz, args.qbits, args.q_vmin, args.q_scale, s),
+                   "query encode");
+        vals = codes;
+    }
+    auto* hid = static_cast<int32_t*>(ws.pinned(Workspace::kIds, ids.size() * sizeof(int32_t) + 4));
+    std::memcpy(hid, ids.data(), ids.size() * sizeof(int32_t));
+    auto* did = static_cast<int32_t*>(ws.dev(Workspace::kIds, ids.size() * sizeof(int32_t) + 4));
+    cuda_check(cudaMemcpyAsync(did, hid, ids.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s),
+               "H2D ids");
+    const size_t cnt = static_cast<size_t>(q.n) * args.k;
+    auto* dd = static_cast<float*>(ws.dev(Workspace::kOutD, cnt * sizeof(float)));
+    auto* dl = static_cast<int32_t*>(ws.dev(Workspace::kOutL, cnt * sizeof(int32_t)));
+    QueryView qv;
+    qv.n = q.n;
+    qv.indptr = u.indptr;
+    qv.idx = u.idx;
+    qv.val = vals;
+    cuda_check(launch_exact_list(val_kind_of(args.qbits), fwd.view(), qv, did,
+                                 static_cast<int>(ids.size()), args.k, args.decode_scale,
+                                 std::max(q.max_nnz, 1), dd, dl, s),
+               "exact list launch");
+    download_results(ws, q.n, args.k, dd, dl, out_d, out_l);
+}
+
+}  // namespace nsp

@@ -1,0 +1,230 @@
+// Host-side engine internals: device buffers, per-thread streams and scratch,
+// the device-resident forward index and SEISMIC lists, and the search drivers
+// that launch the kernels of search_*.cu. Internal to libnsparse_b200.so.
+#ifndef NSP_ENGINE_H
+#define NSP_ENGINE_H
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "nsp_device.h"
+
+namespace nsp {
+
+// Throws std::runtime_error("CUDA error in <what>: <name>") on failure.
+void cuda_check(cudaError_t e, const char* what);
+
+int device_sm_count();
+
+// Owning device array (cudaMalloc / cudaFree).
+template <class T>
+class DevArray {
+public:
+    DevArray() = default;
+    explicit DevArray(size_t n) { resize(n); }
+    ~DevArray() { reset(); }
+    DevArray(const DevArray&) = delete;
+    DevArray& operator=(const DevArray&) = delete;
+    DevArray(DevArray&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr; o.n_ = 0; }
+    DevArray& operator=(DevArray&& o) noexcept {
+        if (this != &o) {
+            reset();
+            p_ = o.p_;
+            n_ = o.n_;
+            o.p_ = nullptr;
+            o.n_ = 0;
+        }
+        return *this;
+    }
+    void resize(size_t n) {
+        reset();
+        if (n > 0) {
+            void* p = nullptr;
+            cuda_check(cudaMalloc(&p, n * sizeof(T)), "cudaMalloc");
+            p_ = static_cast<T*>(p);
+            n_ = n;
+        }
+    }
+    void reset() {
+        if (p_ != nullptr) cudaFree(p_);
+        p_ = nullptr;
+        n_ = 0;
+    }
+    void upload(const T* h, size_t n, cudaStream_t s) {
+        if (n_ < n) resize(n);
+        if (n > 0)
+            cuda_check(cudaMemcpyAsync(p_, h, n * sizeof(T), cudaMemcpyHostToDevice, s), "H2D");
+    }
+    void download(T* h, size_t n, cudaStream_t s) const {
+        if (n > 0)
+            cuda_check(cudaMemcpyAsync(h, p_, n * sizeof(T), cudaMemcpyDeviceToHost, s), "D2H");
+    }
+    T* data() { return p_; }
+    const T* data() const { return p_; }
+    size_t size() const { return n_; }
+
+private:
+    T* p_ = nullptr;
+    size_t n_ = 0;
+};
+
+// Per-thread stream plus grow-only device and pinned scratch, so concurrent
+// searches from several host threads never share buffers (the reference's
+// per-thread scratch, seismic_index.cpp:197-201).
+class Workspace {
+public:
+    enum Slot : int {
+        kQIndptr, kQIdx, kQVal, kQCode, kOutD, kOutL, kSel, kBScore, kCounter, kStats,
+        kCandD, kCandL, kHeapD, kHeapL, kQValG, kIds, kNumSlots
+    };
+    static Workspace& get();
+    cudaStream_t stream() const { return stream_; }
+    void* dev(Slot s, size_t bytes);
+    void* pinned(Slot s, size_t bytes);
+    ~Workspace();
+
+private:
+    Workspace();
+    cudaStream_t stream_ = nullptr;
+    int device_ = 0;
+    void* dptr_[kNumSlots] = {};
+    size_t dcap_[kNumSlots] = {};
+    void* hptr_[kNumSlots] = {};
+    size_t hcap_[kNumSlots] = {};
+};
+
+// Host CSR in the reference's SparseVectors layout (sparse_vectors.h:23-111):
+// int32 row offsets, uint16 terms, values as raw bytes of width esz.
+struct HostCsr {
+    int dim = 0;
+    int esz = 4;
+    std::vector<int32_t> indptr{0};
+    std::vector<uint16_t> indices;
+    std::vector<uint8_t> values;
+
+    int64_t n() const { return static_cast<int64_t>(indptr.size()) - 1; }
+    int64_t nnz() const { return indptr.back(); }
+    // SparseVectors::add_vectors (sparse_vectors.cpp:92-126): append and rebase.
+    void append(int32_t n, const int32_t* ip, const uint16_t* idx, const uint8_t* vals);
+};
+
+class ForwardDevice {
+public:
+    // Builds the padded layout (nsp_device.h) and uploads it.
+    void upload(const HostCsr& h);
+    FwdView view() const;
+    bool empty() const { return n_docs_ == 0; }
+    int32_t n_docs() const { return n_docs_; }
+    int esz() const { return esz_; }
+    size_t device_bytes() const;
+
+private:
+    int32_t n_docs_ = 0;
+    int dim_ = 0;
+    int esz_ = 4;
+    DevArray<uint2> rowinfo_;
+    DevArray<uint16_t> idx_;
+    DevArray<uint8_t> val_;
+};
+
+// SEISMIC lists flattened over terms, in host memory (the reference's
+// InvertedListClusters fields per list, cluster/inverted_list_clusters.h:75-84).
+struct SeismicHost {
+    int esz = 4;
+    std::vector<int64_t> lbp{0};     // blocks per list (prefix)
+    std::vector<int64_t> bdp{0};     // docs per block (prefix)
+    std::vector<int32_t> docs;
+    std::vector<int64_t> ltp{0};     // summary columns per list (prefix)
+    std::vector<uint16_t> sterm;     // column term, ascending within a list
+    std::vector<int64_t> srun{0};    // entries per column (prefix)
+    std::vector<uint16_t> sblk;      // block id local to the list
+    std::vector<uint8_t> sval;       // value bytes, width esz
+    int32_t n_lists() const { return static_cast<int32_t>(lbp.size()) - 1; }
+};
+
+class SeismicDevice {
+public:
+    void upload(const SeismicHost& h, int dim);
+    void download(SeismicHost& h) const;
+    SeismicView view() const;
+    bool empty() const { return n_lists_ == 0; }
+    int32_t max_blocks() const { return max_blocks_; }
+    size_t device_bytes() const;
+
+private:
+    friend struct SeismicBuilder;
+    int32_t n_lists_ = 0;
+    int32_t words_ = 0;
+    int32_t max_blocks_ = 0;
+    int esz_ = 4;
+    DevArray<int64_t> lbp_, bdp_, ltp_, srun_;
+    DevArray<uint16_t> sterm_;
+    DevArray<int32_t> docs_;
+    DevArray<uint2> lmeta_;
+    DevArray<uint16_t> sblk_;
+    DevArray<uint8_t> sval_;
+};
+
+// A host query batch in canonical form (terms ascending and unique per row;
+// a repeated term keeps its last value, as the reference's dense scatter
+// does, sparse_vectors.cpp:157-177).
+struct QueryBatch {
+    int32_t n = 0;
+    std::vector<int32_t> indptr;
+    std::vector<uint16_t> idx;
+    std::vector<float> val;
+    int32_t max_nnz = 0;
+    const int32_t* ip = nullptr;     // points at the caller's arrays when
+    const uint16_t* ix = nullptr;    // they are canonical already
+    const float* vv = nullptr;
+};
+QueryBatch canonicalize(int32_t n, const int32_t* indptr, const uint16_t* idx, const float* val,
+                        int dim);
+
+struct SearchStats {
+    unsigned long long docs_scored = 0;
+    unsigned long long blocks_visited = 0;
+    unsigned long long bytes = 0;
+    unsigned long long lists_probed = 0;
+    float kernel_ms = 0.0f;
+    int launches = 0;
+};
+
+struct SeismicSearchArgs {
+    int k = 10;
+    int cut = 10;
+    float heap_factor = 1.0f;
+    int qbits = 0;            // 0: fp32 index; 8/16: quantized index
+    float q_vmin = 0.0f;      // query quantizer
+    float q_scale = 0.0f;     // kMax / (vmax - vmin) of the query quantizer
+    float decode_scale = 0.0f;
+    bool plain = false;       // one query per launch
+    int warps_per_block = 0;  // 0 = autotuned
+};
+
+// Host buffers in, host buffers out (the reference-facing path).
+void seismic_search(const ForwardDevice& fwd, const SeismicDevice& ix, const QueryBatch& q,
+                    const SeismicSearchArgs& args, const std::vector<uint64_t>* sel_bits,
+                    float* out_d, int32_t* out_l, SearchStats* stats);
+
+void exact_search(const ForwardDevice& fwd, const QueryBatch& q, int k, int mode,
+                  const std::vector<uint64_t>* sel_bits, float* out_d, int32_t* out_l,
+                  SearchStats* stats);
+
+void exact_list_search(const ForwardDevice& fwd, const QueryBatch& q, const SeismicSearchArgs& args,
+                       const std::vector<int32_t>& ids, float* out_d, int32_t* out_l);
+
+// Device-resident variant: queries, outputs and stream owned by the caller.
+void seismic_search_device(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
+                           const int32_t* d_indptr, const uint16_t* d_idx, const void* d_val,
+                           int32_t max_nnz, const SeismicSearchArgs& args, const uint64_t* d_sel,
+                           float* d_out, int32_t* d_lab, cudaStream_t s, SearchStats* stats);
+
+}  // namespace nsp
+
+#endif  // NSP_ENGINE_H

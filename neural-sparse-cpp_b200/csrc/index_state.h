@@ -1,0 +1,62 @@
+// Internal state behind the nsparse index classes: the host copy of the
+// forward index (kept for persistence and rebuilds), its device image, and
+// the SEISMIC lists on host and device.
+#ifndef NSP_INDEX_STATE_H
+#define NSP_INDEX_STATE_H
+
+#include <cstdint>
+#include <mutex>
+#include <vector>
+
+#include "engine.h"
+#include "nsparse/id_selector.h"
+#include "nsparse/index.h"
+#include "nsparse/seismic_index.h"
+
+namespace nsparse {
+namespace detail {
+
+struct ForwardState {
+    ForwardState(int dim, int esz) {
+        host.dim = dim;
+        host.esz = esz;
+    }
+    nsp::HostCsr host;
+    nsp::ForwardDevice dev;
+    bool dirty = true;
+    std::mutex mu;
+    void append(idx_t n, const idx_t* indptr, const term_t* indices, const uint8_t* value_bytes);
+    void ensure_device();
+    bool terms_in_range(int dim) const;
+};
+
+struct SeismicState {
+    SeismicState(int dim, int esz) : vectors(dim, esz) { lists.esz = esz; }
+    ForwardState vectors;
+    nsp::SeismicHost lists;          // host copy, valid when host_valid
+    std::vector<uint8_t> list_esz;   // element width each list declares on disk
+    nsp::SeismicDevice lists_dev;
+    bool host_valid = false;
+    bool dev_valid = false;
+    std::mutex mu;
+    // Uploads the host lists if the device copy is stale.
+    void ensure_lists();
+    // Host copy of the lists (downloaded after a device build).
+    const nsp::SeismicHost& host_lists();
+};
+
+// SEISMIC build on the device (seismic_build.cu).
+void seismic_build(SeismicState& st, int dim, const SeismicClusterParameters& params);
+
+std::vector<uint64_t> selector_bitmap(const IDSelector* sel, int64_t n_docs);
+
+// SEISMIC search over device-resident queries and results (nsparse_c.h,
+// nsp_index_search_device). Enqueues on `s` and returns.
+void search_device(Index* index, int32_t n, const int32_t* d_indptr, const uint16_t* d_idx,
+                   const float* d_val, int32_t max_nnz, int k, float* d_out, int32_t* d_lab,
+                   SearchParameters* params, cudaStream_t s);
+
+}  // namespace detail
+}  // namespace nsparse
+
+#endif  // NSP_INDEX_STATE_H

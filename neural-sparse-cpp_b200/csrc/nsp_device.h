@@ -1,0 +1,137 @@
+// Device-side data layouts and kernel launchers of the B200 sparse-retrieval
+// engine. Everything here is internal to libnsparse_b200.so; the public
+// surface is include/nsparse_c.h (C ABI) and include/nsparse/*.h (C++ API).
+//
+// HBM layouts
+// -----------
+// Forward index (the reference's SparseVectors CSR, sparse_vectors.h:36-111)
+//   rowinfo[d] = {start / 16, length}: row d's elements begin at element
+//   16*rowinfo[d].x of `idx` (uint16 term ids) and `val` (float32, uint8 or
+//   uint16 codes). Every row starts on a 16-element boundary and is padded to
+//   a multiple of 16 elements, so a row is read with aligned 16-byte vector
+//   loads (idx: 32-byte rows starts, fp32 values: 64-byte) and a lane never
+//   reads past its row's padding.
+//
+// SEISMIC index (the reference's InvertedListClusters per term,
+// cluster/inverted_list_clusters.h:75-84), flattened over the lists:
+//   list t owns blocks [lbp[t], lbp[t+1]); block b owns docs[bdp[b]..bdp[b+1]).
+//   Summaries are term-major (CSC) per list: summary column c of list t is the
+//   term whose bit is set in the list's term bitmap `lmeta`; its (block, value)
+//   run is sblk/sval[srun[ltp[t]+c] .. srun[ltp[t]+c+1]).
+//   lmeta[t*W + w] = {bits of terms 32w..32w+31 present in list t's summaries,
+//   number of present terms below 32w}. A query term is located in a list with
+//   one 8-byte load and a popcount, instead of the reference's binary search
+//   over term_ids (inverted_list_clusters.cpp:302-304).
+#ifndef NSP_DEVICE_H
+#define NSP_DEVICE_H
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace nsp {
+
+constexpr int kRowAlign = 16;  // elements
+
+enum ValKind : int { kF32 = 4, kU8 = 1, kU16 = 2 };
+
+struct FwdView {
+    int32_t n_docs;
+    int32_t dim;
+    const uint2* rowinfo;
+    const uint16_t* idx;
+    const void* val;
+};
+
+struct SeismicView {
+    int32_t n_lists;
+    int32_t words;          // ceil(dim / 32)
+    int32_t max_blocks;     // max blocks in one list
+    const int64_t* lbp;     // [n_lists + 1]
+    const int64_t* bdp;     // [n_blocks + 1]
+    const int32_t* docs;    // [n_list_docs]
+    const uint2* lmeta;     // [n_lists * words]
+    const int64_t* ltp;     // [n_lists + 1], column base per list
+    const int64_t* srun;    // [n_columns + 1]
+    const uint16_t* sblk;   // [n_entries]
+    const void* sval;       // [n_entries], float32 / uint8 / uint16
+};
+
+// A query batch in canonical form: each row's terms ascending and unique.
+struct QueryView {
+    int32_t n;
+    const int32_t* indptr;
+    const uint16_t* idx;
+    const void* val;        // same element type as the index values
+};
+
+// Counters the search kernels accumulate (unsigned long long each).
+enum StatSlot : int {
+    kStatDocsScored = 0,
+    kStatBlocksVisited = 1,
+    kStatBytes = 2,
+    kStatListsProbed = 3,
+    kStatCount = 4,
+};
+
+struct SeismicLaunch {
+    FwdView fwd;
+    SeismicView ix;
+    QueryView q;
+    int k;
+    int cut;
+    float heap_factor;
+    float decode_scale;         // SQ: quantized score -> float (0 = none)
+    const uint64_t* sel_bits;   // doc bitmap or nullptr
+    float* out_d;
+    int32_t* out_l;
+    int32_t qcap;               // max query nnz in the batch
+    int32_t* work_counter;      // work stealing over queries, or nullptr
+    float* bscore;              // scratch: per warp slot, max_blocks floats
+    unsigned long long* stats;  // kStatCount counters, or nullptr
+    int32_t first_query;        // static mode: queries first_query.. strided
+};
+
+struct ExactLaunch {
+    FwdView fwd;
+    QueryView q;
+    int k;
+    int mode;                   // 0 brutal (all docs), 1 inverted (score > 0)
+    const uint64_t* sel_bits;   // honoured in mode 1
+    int32_t qcap;
+    float* qval_global;         // query values in global scratch, or nullptr
+    int32_t docs_per_tile;
+    float* cand_d;              // scratch [n_q][tiles][k]
+    int32_t* cand_l;
+    float* heap_d;              // scratch per (tile, group, warp, lane) k
+    int32_t* heap_l;
+    float* out_d;
+    int32_t* out_l;
+    unsigned long long* stats;
+};
+
+// Launchers (return cudaError_t of the launch). `sm_count` sizes persistent
+// grids; `plan_*` report the dynamic shared memory a launch needs.
+size_t seismic_smem_per_warp(int val_kind, int dim_words, int qcap, int k);
+cudaError_t launch_seismic(int val_kind, const SeismicLaunch& a, int warps_per_block,
+                           int blocks, cudaStream_t s);
+int seismic_max_blocks_per_sm(int val_kind, int warps_per_block, size_t smem);
+
+size_t exact_smem(int dim_words, int qcap_smem);  // qcap_smem 0: values in global
+cudaError_t launch_exact(const ExactLaunch& a, int tiles, cudaStream_t s);
+
+// Exact scoring of an explicit doc list per query (the reference's
+// ExactMatcher, exact_matcher.h:23-58): ids ascending, at most k of them.
+cudaError_t launch_exact_list(int val_kind, const FwdView& fwd, const QueryView& q,
+                              const int32_t* ids, int n_ids, int k, float decode_scale,
+                              int32_t qcap, float* out_d, int32_t* out_l,
+                              cudaStream_t s);
+
+// ScalarQuantizer::encode (utils/scalar_quantizer.h:97-118) on the device.
+cudaError_t launch_sq_encode(const float* vals, void* codes, int64_t n, int qbits,
+                             float vmin, float inv_range_scaled, cudaStream_t s);
+
+}  // namespace nsp
+
+#endif  // NSP_DEVICE_H

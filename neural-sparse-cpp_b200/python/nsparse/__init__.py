@@ -1,0 +1,364 @@
+"""nsparse: the reference library's Python API over the B200 engine.
+
+Mirrors the SWIG module of opensearch-project/neural-sparse-cpp
+(nsparse/python/swignsparse.swig, class_wrappers.py): ``index_factory``,
+``Index.add / add_with_ids / build / search / num_vectors / get_dimension``,
+``SearchParameters`` and its SEISMIC subclasses, the id selectors,
+``write_index / read_index`` and ``kUseMmap``. Search returns
+``(distances, labels)`` as ``(n, k)`` float32 / int32 arrays.
+
+Everything goes through the C ABI of ``lib/libnsparse_b200.so``
+(include/nsparse_c.h); the library must be built first
+(``python neural-sparse-cpp_b200/build.py``). C++ exceptions arrive as the
+Python exceptions the reference's SWIG layer raises: ValueError, RuntimeError,
+IndexError, MemoryError.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+__version__ = "0.1.0"
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.abspath(os.path.join(_HERE, "..", "..", "lib", "libnsparse_b200.so"))
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"nsparse engine library not found at {LIB_PATH}; build it with "
+        "`python neural-sparse-cpp_b200/build.py`")
+
+_L = ctypes.CDLL(LIB_PATH)
+_P = ctypes.c_void_p
+_I32 = ctypes.c_int32
+
+
+def _sig(name, *argtypes):
+    f = getattr(_L, name)
+    f.restype = ctypes.c_int
+    f.argtypes = list(argtypes)
+    return f
+
+
+_L.nsp_last_error.restype = ctypes.c_char_p
+_L.nsp_last_error.argtypes = []
+_sig("nsp_index_factory", ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(_P))
+_sig("nsp_index_free", _P)
+_sig("nsp_index_add", _P, _I32, _P, _P, _P)
+_sig("nsp_index_add_with_ids", _P, _I32, _P, _P, _P, _P)
+_sig("nsp_index_build", _P)
+_sig("nsp_index_search", _P, _I32, _P, _P, _P, ctypes.c_int, _P, _P, _P)
+_sig("nsp_index_num_vectors", _P, ctypes.POINTER(ctypes.c_int64))
+_sig("nsp_index_dimension", _P, ctypes.POINTER(_I32))
+_sig("nsp_index_fourcc", _P, ctypes.c_char_p)
+_sig("nsp_index_read_csr", _P, ctypes.c_char_p, ctypes.c_int)
+_sig("nsp_write_index", _P, ctypes.c_char_p)
+_sig("nsp_read_index", ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(_P))
+_sig("nsp_id_selector_set_new", ctypes.c_size_t, _P, ctypes.POINTER(_P))
+_sig("nsp_id_selector_array_new", ctypes.c_size_t, _P, ctypes.POINTER(_P))
+_sig("nsp_id_selector_not_new", _P, ctypes.POINTER(_P))
+_sig("nsp_id_selector_bitmap_new", ctypes.c_int64, _P, ctypes.POINTER(_P))
+_sig("nsp_id_selector_is_member", _P, _I32, ctypes.POINTER(ctypes.c_int))
+_sig("nsp_id_selector_free", _P)
+_sig("nsp_search_params_new", ctypes.POINTER(_P))
+_sig("nsp_seismic_search_params_new", ctypes.c_int, ctypes.c_float, ctypes.POINTER(_P))
+_sig("nsp_seismic_sq_search_params_new", ctypes.c_float, ctypes.c_float, ctypes.c_int,
+     ctypes.c_float, ctypes.POINTER(_P))
+_sig("nsp_search_params_set_id_selector", _P, _P)
+_sig("nsp_search_params_set_engine", _P, ctypes.c_int, ctypes.c_int)
+_sig("nsp_search_params_free", _P)
+_sig("nsp_index_search_device", _P, _I32, _P, _P, _P, _I32, ctypes.c_int, _P, _P, _P, _P)
+_sig("nsp_device_info", ctypes.POINTER(_I32), ctypes.c_char_p, ctypes.c_size_t)
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("docs_scored", ctypes.c_uint64), ("blocks_visited", ctypes.c_uint64),
+                ("bytes", ctypes.c_uint64), ("lists_probed", ctypes.c_uint64),
+                ("kernel_ms", ctypes.c_float), ("launches", ctypes.c_int32)]
+
+
+_sig("nsp_last_search_stats", ctypes.POINTER(_Stats))
+
+_ERRORS = {1: ValueError, 2: RuntimeError, 3: IndexError, 4: MemoryError}
+
+kUseMmap = 1
+
+
+def _check(rc):
+    if rc != 0:
+        msg = _L.nsp_last_error().decode(errors="replace")
+        raise _ERRORS.get(rc, RuntimeError)(msg)
+
+
+def _ptr(a):
+    return a.ctypes.data if a is not None else None
+
+
+def _typed(a, dtype, name):
+    """Buffer check of the reference's typemaps: a wrong dtype is an error."""
+    a = np.asarray(a)
+    if a.dtype != np.dtype(dtype):
+        raise TypeError(f"Expected {np.dtype(dtype).name} array for {name}")
+    return np.ascontiguousarray(a)
+
+
+# ------------------------------------------------------------ selectors --
+
+class IDSelector:
+    """Base of the id selectors (reference: nsparse/id_selector.h:22-86)."""
+
+    _h = None
+
+    def is_member(self, id_):
+        out = ctypes.c_int()
+        _check(_L.nsp_id_selector_is_member(self._h, int(id_), ctypes.byref(out)))
+        return bool(out.value)
+
+    def __call__(self, id_):
+        return self.is_member(id_)
+
+    def __del__(self):
+        h, self._h = self._h, None
+        if h:
+            _L.nsp_id_selector_free(h)
+
+
+class SetIDSelector(IDSelector):
+    def __init__(self, ids):
+        ids = _typed(ids, np.int32, "indices")
+        h = _P()
+        _check(_L.nsp_id_selector_set_new(len(ids), _ptr(ids), ctypes.byref(h)))
+        self._h = h.value
+
+
+class ArrayIDSelector(IDSelector):
+    def __init__(self, ids):
+        ids = _typed(ids, np.int32, "indices")
+        h = _P()
+        _check(_L.nsp_id_selector_array_new(len(ids), _ptr(ids), ctypes.byref(h)))
+        self._h = h.value
+
+
+class NotIDSelector(IDSelector):
+    def __init__(self, selector):
+        h = _P()
+        _check(_L.nsp_id_selector_not_new(selector._h, ctypes.byref(h)))
+        self._h = h.value
+        self._inner = selector  # the C++ object borrows it
+
+
+class BitmapIDSelector(IDSelector):
+    """Extension: membership bitmap over ids [0, n_bits), bit d of word d // 64."""
+
+    def __init__(self, n_bits, bits):
+        bits = _typed(bits, np.uint64, "bits")
+        if len(bits) * 64 < n_bits:
+            raise ValueError("bitmap shorter than n_bits")
+        h = _P()
+        _check(_L.nsp_id_selector_bitmap_new(int(n_bits), _ptr(bits), ctypes.byref(h)))
+        self._h = h.value
+
+
+# ----------------------------------------------------------- parameters --
+
+class SearchParameters:
+    """Reference: nsparse/index.h:21-28."""
+
+    def __init__(self):
+        h = _P()
+        _check(_L.nsp_search_params_new(ctypes.byref(h)))
+        self._h = h.value
+        self._sel = None
+
+    def set_id_selector(self, selector):
+        _check(_L.nsp_search_params_set_id_selector(self._h, None if selector is None else selector._h))
+        self._sel = selector
+
+    def get_id_selector(self):
+        return self._sel
+
+    def set_engine(self, plain=False, warps_per_block=0):
+        """Extension: plain=True runs one kernel launch per query."""
+        _check(_L.nsp_search_params_set_engine(self._h, int(bool(plain)), int(warps_per_block)))
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            _L.nsp_search_params_free(h)
+
+
+class SeismicSearchParameters(SearchParameters):
+    """Reference: nsparse/seismic_index.h:26-32 (cut=10, heap_factor=1.0)."""
+
+    def __init__(self, cut=10, heap_factor=1.0):
+        h = _P()
+        _check(_L.nsp_seismic_search_params_new(int(cut), float(heap_factor), ctypes.byref(h)))
+        self._h = h.value
+        self._sel = None
+        self.cut = int(cut)
+        self.heap_factor = float(heap_factor)
+
+
+class SeismicSQSearchParameters(SeismicSearchParameters):
+    """Reference: nsparse/seismic_scalar_quantized_index.h:27-33."""
+
+    def __init__(self, vmin, vmax, cut=10, heap_factor=1.0):
+        h = _P()
+        _check(_L.nsp_seismic_sq_search_params_new(float(vmin), float(vmax), int(cut),
+                                                   float(heap_factor), ctypes.byref(h)))
+        self._h = h.value
+        self._sel = None
+        self.vmin = float(vmin)
+        self.vmax = float(vmax)
+        self.cut = int(cut)
+        self.heap_factor = float(heap_factor)
+
+
+# ---------------------------------------------------------------- index --
+
+class Index:
+    """Reference: nsparse/index.h:30-68 with the SWIG search wrapper
+    (class_wrappers.py:22-58)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    def add(self, n, indptr, indices, values):
+        indptr = _typed(indptr, np.int32, "indptr")
+        indices = _typed(indices, np.uint16, "indices")
+        values = _typed(values, np.float32, "values")
+        _check(_L.nsp_index_add(self._h, int(n), _ptr(indptr), _ptr(indices), _ptr(values)))
+
+    def add_with_ids(self, n, indptr, indices, values, ids):
+        indptr = np.ascontiguousarray(indptr, dtype=np.int32)
+        indices = np.ascontiguousarray(indices, dtype=np.uint16)
+        values = np.ascontiguousarray(values, dtype=np.float32)
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        _check(_L.nsp_index_add_with_ids(self._h, int(n), _ptr(indptr), _ptr(indices),
+                                         _ptr(values), _ptr(ids)))
+
+    def build(self):
+        _check(_L.nsp_index_build(self._h))
+
+    def search(self, n, indptr, indices, values, k, params=None):
+        indptr = np.ascontiguousarray(indptr, dtype=np.int32)
+        indices = np.ascontiguousarray(indices, dtype=np.uint16)
+        values = np.ascontiguousarray(values, dtype=np.float32)
+        n, k = int(n), int(k)
+        if n <= 0 or k <= 0:
+            # same message the C++ layer gives; allocation below needs n, k > 0
+            raise ValueError("value must be positive")
+        distances = np.empty((n, k), dtype=np.float32)
+        labels = np.empty((n, k), dtype=np.int32)
+        _check(_L.nsp_index_search(self._h, n, _ptr(indptr), _ptr(indices), _ptr(values), k,
+                                   _ptr(distances), _ptr(labels),
+                                   None if params is None else params._h))
+        return distances, labels
+
+    def search_device(self, n, d_indptr, d_indices, d_values, max_row_nnz, k, d_distances,
+                      d_labels, params=None, stream=None):
+        """Extension: device pointers in and out (ints), enqueued on `stream`."""
+        _check(_L.nsp_index_search_device(self._h, int(n), d_indptr, d_indices, d_values,
+                                          int(max_row_nnz), int(k), d_distances, d_labels,
+                                          None if params is None else params._h, stream))
+
+    def num_vectors(self):
+        out = ctypes.c_int64()
+        _check(_L.nsp_index_num_vectors(self._h, ctypes.byref(out)))
+        return out.value
+
+    def get_dimension(self):
+        out = _I32()
+        _check(_L.nsp_index_dimension(self._h, ctypes.byref(out)))
+        return out.value
+
+    def id(self):
+        buf = ctypes.create_string_buffer(4)
+        _check(_L.nsp_index_fourcc(self._h, buf))
+        return buf.raw.decode()
+
+    def read_csr(self, file_path, residency=0):
+        _check(_L.nsp_index_read_csr(self._h, str(file_path).encode(), int(residency)))
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            _L.nsp_index_free(h)
+
+
+class BrutalIndex(Index):
+    pass
+
+
+class InvertedIndex(Index):
+    pass
+
+
+class SeismicIndex(Index):
+    pass
+
+
+class SeismicScalarQuantizedIndex(Index):
+    pass
+
+
+class IDMapIndex(Index):
+    pass
+
+
+_BY_FOURCC = {"BRUT": BrutalIndex, "INVT": InvertedIndex, "SEIS": SeismicIndex,
+              "SESQ": SeismicScalarQuantizedIndex, "IDMP": IDMapIndex}
+
+
+def _wrap(handle):
+    idx = Index(handle)
+    cls = _BY_FOURCC.get(idx.id(), Index)
+    idx.__class__ = cls
+    return idx
+
+
+def index_factory(dim, description):
+    """Reference: nsparse/index_factory.cpp:63-153."""
+    h = _P()
+    desc = description.encode() if description is not None else None
+    _check(_L.nsp_index_factory(int(dim), desc, ctypes.byref(h)))
+    return _wrap(h.value)
+
+
+def write_index(index, file_name):
+    _check(_L.nsp_write_index(index._h, str(file_name).encode()))
+
+
+def read_index(file_name, io_flags=0):
+    h = _P()
+    _check(_L.nsp_read_index(str(file_name).encode(), int(io_flags), ctypes.byref(h)))
+    return _wrap(h.value)
+
+
+@dataclass
+class SearchStats:
+    docs_scored: int
+    blocks_visited: int
+    bytes: int
+    lists_probed: int
+    kernel_ms: float
+    launches: int
+
+
+def last_search_stats() -> SearchStats:
+    """Extension: work counters and device time of this thread's last search."""
+    s = _Stats()
+    _check(_L.nsp_last_search_stats(ctypes.byref(s)))
+    return SearchStats(s.docs_scored, s.blocks_visited, s.bytes, s.lists_probed, s.kernel_ms,
+                       s.launches)
+
+
+def device_info():
+    n = _I32()
+    buf = ctypes.create_string_buffer(256)
+    _check(_L.nsp_device_info(ctypes.byref(n), buf, 256))
+    return n.value, buf.value.decode()

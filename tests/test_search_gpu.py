@@ -1,0 +1,289 @@
+"""GPU parity: every search path through the C ABI against the oracle and the
+reference's golden results.
+
+Tolerances: BrutalIndex / InvertedIndex / SEISMIC fp32 scores are bit-identical
+to the oracle (the kernels sum in the reference's order); InvertedIndex scores
+are within 1e-5 relative of the reference's own MaxScore sums; SEISMIC ids and
+scores equal the oracle's bit for bit; SEISMIC-SQ integer code sums are exact.
+"""
+
+import numpy as np
+import pytest
+
+import nsparse
+import oracle as O
+from helpers import CUT, HF, K, SEISMIC, golden, golden_corpus, oracle_seismic_from_file, recall, \
+    ref_file, sq_exact_scores, sq_spec
+from nsparse_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def make(spec, docs, build=True, ids=None):
+    idx = nsparse.index_factory(docs.dim, spec)
+    if ids is None:
+        idx.add(docs.n, docs.indptr, docs.indices, docs.values)
+    else:
+        idx.add_with_ids(docs.n, docs.indptr, docs.indices, docs.values, ids)
+    if build:
+        idx.build()
+    return idx
+
+
+def search(idx, qs, k=K, params=None):
+    return idx.search(qs.n, qs.indptr, qs.indices, qs.values, k, params)
+
+
+def search_each(idx, qs, k=K, params=None):
+    D = np.empty((qs.n, k), np.float32)
+    L = np.empty((qs.n, k), np.int32)
+    for q in range(qs.n):
+        r = qs.rows(q, q + 1)
+        D[q], L[q] = search(idx, r, k, params)
+    return D, L
+
+
+# ------------------------------------------------------------- exact -------
+
+def test_brutal_matches_reference_golden():
+    g = golden()
+    docs, qs = golden_corpus()
+    idx = make("brutal", docs, build=False)
+    D, L = search(idx, qs)
+    np.testing.assert_array_equal(L, g["brutal_L"])
+    np.testing.assert_array_equal(D, g["brutal_D"])
+    assert nsparse.last_search_stats().launches >= 1
+
+
+def test_inverted_matches_reference_golden():
+    g = golden()
+    docs, qs = golden_corpus()
+    idx = make("inverted", docs)
+    D, L = search(idx, qs)
+    np.testing.assert_array_equal(L, g["inverted_L"])
+    np.testing.assert_allclose(D, g["inverted_D"], rtol=1e-5, atol=1e-6)
+    Do, Lo = O.exact_search(docs, qs, K, 1)
+    np.testing.assert_array_equal(D, Do)
+
+
+def test_inverted_filter_matches_reference_golden():
+    g = golden()
+    docs, qs = golden_corpus()
+    idx = make("inverted", docs)
+    p = nsparse.SearchParameters()
+    p.set_id_selector(nsparse.SetIDSelector(g["filter_ids"]))
+    D, L = search(idx, qs, params=p)
+    np.testing.assert_array_equal(L, g["inv_filter_L"])
+    np.testing.assert_allclose(D, g["inv_filter_D"], rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.parametrize("k", [1, 10, 37, 100])
+def test_exact_paths_match_oracle_medium(k):
+    docs = synth.docs_config0(30000, seed=5)
+    qs = synth.queries_config0(150, seed=5)
+    b = make("brutal", docs, build=False)
+    D, L = search(b, qs, k)
+    Do, Lo = O.exact_search(docs, qs, k, 0)
+    np.testing.assert_array_equal(L, Lo)
+    np.testing.assert_array_equal(D, Do)
+    v = make("inverted", docs)
+    D, L = search(v, qs, k)
+    Do, Lo = O.exact_search(docs, qs, k, 1)
+    np.testing.assert_array_equal(L, Lo)
+    np.testing.assert_array_equal(D, Do)
+
+
+def test_brutal_ignores_selector_and_pads():
+    docs, qs = golden_corpus()
+    idx = make("brutal", docs, build=False)
+    p = nsparse.SearchParameters()
+    p.set_id_selector(nsparse.SetIDSelector(np.arange(50, dtype=np.int32)))
+    _, L1 = search(idx, qs, params=p)
+    _, L0 = search(idx, qs)
+    np.testing.assert_array_equal(L1, L0)
+    small = make("brutal", docs.rows(0, 3), build=False)
+    D, L = search(small, qs, 10)
+    assert (L[:, 3:] == -1).all() and (D[:, 3:] == -1.0).all()
+
+
+def test_inverted_not_selector_and_short_rows():
+    docs, qs = golden_corpus()
+    idx = make("inverted", docs)
+    _, L0 = search(idx, qs)
+    banned = L0[:, :3].ravel()
+    p = nsparse.SearchParameters()
+    inner = nsparse.SetIDSelector(banned.astype(np.int32))
+    p.set_id_selector(nsparse.NotIDSelector(inner))
+    _, L = search(idx, qs, params=p)
+    assert not np.isin(L[L >= 0], banned).any()
+    Do, Lo = O.exact_search(docs, qs, K, 1, sel_bits=~O.bitmap_from_ids(docs.n, banned))
+    np.testing.assert_array_equal(L, Lo)
+
+
+# ----------------------------------------------------------- SEISMIC ------
+
+@pytest.fixture(scope="module")
+def seismic_file(tmp_path_factory):
+    docs, _ = golden_corpus()
+    p = tmp_path_factory.mktemp("idx") / "s.idx"
+    ref_file(docs, SEISMIC, p)
+    return p
+
+
+def test_seismic_matches_reference_golden(seismic_file):
+    g = golden()
+    _, qs = golden_corpus()
+    idx = nsparse.read_index(str(seismic_file))
+    D, L = search(idx, qs, params=nsparse.SeismicSearchParameters(CUT, HF))
+    np.testing.assert_array_equal(L, g["seismic_L"])
+    np.testing.assert_array_equal(D, g["seismic_D"])
+    st = nsparse.last_search_stats()
+    assert st.docs_scored > 0 and st.bytes > 0 and st.launches == 1
+
+
+def test_seismic_plain_equals_batched(seismic_file):
+    _, qs = golden_corpus()
+    idx = nsparse.read_index(str(seismic_file))
+    p = nsparse.SeismicSearchParameters(CUT, HF)
+    Db, Lb = search(idx, qs, params=p)
+    p.set_engine(plain=True)
+    Dp, Lp = search(idx, qs, params=p)
+    assert nsparse.last_search_stats().launches == qs.n
+    np.testing.assert_array_equal(Lp, Lb)
+    np.testing.assert_array_equal(Dp, Db)
+    p2 = nsparse.SeismicSearchParameters(CUT, HF)
+    De, Le = search_each(idx, qs, params=p2)
+    np.testing.assert_array_equal(Le, Lb)
+    np.testing.assert_array_equal(De, Db)
+    for wpb in (1, 2, 8):
+        p3 = nsparse.SeismicSearchParameters(CUT, HF)
+        p3.set_engine(False, wpb)
+        Dw, Lw = search(idx, qs, params=p3)
+        np.testing.assert_array_equal(Lw, Lb)
+        np.testing.assert_array_equal(Dw, Db)
+
+
+def test_seismic_filter_and_exact_path_match_golden(seismic_file):
+    g = golden()
+    _, qs = golden_corpus()
+    idx = nsparse.read_index(str(seismic_file))
+    p = nsparse.SeismicSearchParameters(CUT, HF)
+    p.set_id_selector(nsparse.SetIDSelector(g["filter_ids"]))
+    D, L = search(idx, qs, params=p)
+    np.testing.assert_array_equal(L, g["filter_L"])
+    np.testing.assert_array_equal(D, g["filter_D"])
+    p = nsparse.SeismicSearchParameters(CUT, HF)
+    p.set_id_selector(nsparse.SetIDSelector(g["exact_ids"]))
+    D, L = search(idx, qs.rows(0, 4), params=p)
+    np.testing.assert_array_equal(L, g["exact_L"])
+    np.testing.assert_array_equal(D, g["exact_D"])
+
+
+@pytest.mark.parametrize("cut,hf,k", [(1, 1.0, 10), (3, 0.7, 5), (12, 0.95, 100), (200, 2.0, 10)])
+def test_seismic_matches_oracle_params(seismic_file, cut, hf, k):
+    _, qs = golden_corpus()
+    idx = nsparse.read_index(str(seismic_file))
+    D, L = search(idx, qs, k, nsparse.SeismicSearchParameters(cut, hf))
+    Do, Lo = oracle_seismic_from_file(seismic_file, qs, k, cut, hf)
+    np.testing.assert_array_equal(L, Lo)
+    np.testing.assert_array_equal(D, Do)
+
+
+def test_seismic_medium_corpus_matches_oracle_and_reference(tmp_path):
+    docs = synth.docs_config0(20000, seed=3)
+    qs = synth.queries_config0(300, seed=3)
+    spec = "seismic,lambda=400|beta=40|alpha=0.4|seed=7"
+    r = ref_file(docs, spec, tmp_path / "m.idx")
+    idx = nsparse.read_index(str(tmp_path / "m.idx"))
+    D, L = search(idx, qs, params=nsparse.SeismicSearchParameters(10, 0.8))
+    Do, Lo = oracle_seismic_from_file(tmp_path / "m.idx", qs, K, 10, 0.8)
+    np.testing.assert_array_equal(L, Lo)
+    np.testing.assert_array_equal(D, Do)
+    Dr, Lr = r.search(qs, K, param_kind=2, cut=10, heap_factor=0.8)
+    same = (Lr == L).all(axis=1)
+    assert same.mean() >= 0.99
+    np.testing.assert_array_equal(Dr[same], D[same])
+    _, Lt = O.exact_search(docs, qs, K, 1)
+    assert recall(L, Lt) >= recall(Lr, Lt) - 0.005
+
+
+def test_seismic_sq_matches_oracle_and_scores_exact(tmp_path):
+    g = golden()
+    docs, qs = golden_corpus()
+    vmin, vmax = float(g["sq_vmin"]), float(g["sq_vmax"])
+    ref_file(docs, sq_spec(vmin, vmax), tmp_path / "q.idx")
+    idx = nsparse.read_index(str(tmp_path / "q.idx"))
+    D, L = search(idx, qs, params=nsparse.SeismicSearchParameters(CUT, HF))
+    codes = O.sq_encode_u8(vmin, vmax, qs.values)
+    Do, Lo = oracle_seismic_from_file(tmp_path / "q.idx", qs, K, CUT, HF, codes=codes)
+    scale = np.float32(O.sq_scale(vmin, vmax, vmin, vmax))
+    np.testing.assert_array_equal(L, Lo)
+    np.testing.assert_array_equal(D, np.where(Lo >= 0, (Do * scale).astype(np.float32), Do))
+    exact = sq_exact_scores(docs, codes, qs, L, vmin, vmax) * scale
+    np.testing.assert_array_equal(D[L >= 0], exact[L >= 0])
+    _, Lt = O.exact_search(docs, qs, K, 1)
+    assert recall(L, Lt) >= recall(g["sq_L"], Lt) - 0.02
+
+
+def test_seismic_sq_query_range_override(tmp_path):
+    g = golden()
+    docs, qs = golden_corpus()
+    vmin, vmax = float(g["sq_vmin"]), float(g["sq_vmax"])
+    ref_file(docs, sq_spec(vmin, vmax), tmp_path / "q.idx")
+    idx = nsparse.read_index(str(tmp_path / "q.idx"))
+    qmin, qmax = 0.0, float(qs.values.max())
+    D, L = search(idx, qs, params=nsparse.SeismicSQSearchParameters(qmin, qmax, CUT, HF))
+    codes = O.sq_encode_u8(qmin, qmax, qs.values)
+    Do, Lo = oracle_seismic_from_file(tmp_path / "q.idx", qs, K, CUT, HF, codes=codes)
+    scale = np.float32(O.sq_scale(vmin, vmax, qmin, qmax))
+    np.testing.assert_array_equal(L, Lo)
+    np.testing.assert_array_equal(D, np.where(Lo >= 0, (Do * scale).astype(np.float32), Do))
+
+
+def test_idmap_seismic_returns_external_ids(tmp_path):
+    g = golden()
+    docs, qs = golden_corpus()
+    ext = (np.arange(docs.n, dtype=np.int32) * 7 + 1000)
+    ref_file(docs, "idmap," + SEISMIC, tmp_path / "i.idx", ids=ext)
+    idx = nsparse.read_index(str(tmp_path / "i.idx"))
+    D, L = search(idx, qs, params=nsparse.SeismicSearchParameters(CUT, HF))
+    want = np.where(g["seismic_L"] >= 0, ext[np.maximum(g["seismic_L"], 0)], -1)
+    np.testing.assert_array_equal(L, want)
+    np.testing.assert_array_equal(D, g["seismic_D"])
+    # selector in external ids, translated for the delegate
+    p = nsparse.SeismicSearchParameters(CUT, HF)
+    allowed = ext[g["filter_ids"]]
+    sel = nsparse.SetIDSelector(allowed)
+    p.set_id_selector(sel)
+    D, L = search(idx, qs, params=p)
+    want = np.where(g["filter_L"] >= 0, ext[np.maximum(g["filter_L"], 0)], -1)
+    np.testing.assert_array_equal(L, want)
+    assert p.get_id_selector() is sel
+
+
+def test_search_before_build_is_padding():
+    docs, qs = golden_corpus()
+    idx = nsparse.index_factory(docs.dim, SEISMIC)
+    idx.add(docs.n, docs.indptr, docs.indices, docs.values)
+    D, L = search(idx, qs)
+    assert (L == -1).all() and (D == -1.0).all()
+
+
+def test_unsorted_and_empty_query_rows(seismic_file):
+    docs, qs = golden_corpus()
+    idx = nsparse.read_index(str(seismic_file))
+    p = nsparse.SeismicSearchParameters(CUT, HF)
+    D0, L0 = search(idx, qs, params=p)
+    # reverse each row's term order: canonicalisation restores the same result
+    ip, ix, v = qs.indptr, qs.indices.copy(), qs.values.copy()
+    for q in range(qs.n):
+        s, e = ip[q], ip[q + 1]
+        ix[s:e] = ix[s:e][::-1].copy()
+        v[s:e] = v[s:e][::-1].copy()
+    D1, L1 = idx.search(qs.n, ip, ix, v, K, p)
+    np.testing.assert_array_equal(L1, L0)
+    # an empty row returns padding, its neighbours are unaffected
+    ip2 = np.concatenate([[0], [0], ip[1:3]]).astype(np.int32)
+    D2, L2 = idx.search(3, ip2, qs.indices, qs.values, K, p)
+    assert (L2[0] == -1).all()
+    np.testing.assert_array_equal(L2[1:], L0[:2])
