@@ -470,6 +470,11 @@ void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
     SeismicLaunch a{};
     a.fwd = fwd.view();
     a.ix = ix.view();
+    // The query bitmap spans the vocabulary even when no lists exist (an
+    // unbuilt index), so its width comes from the forward index.
+    a.ix.words = (a.fwd.dim + 31) / 32;
+    if (ix.view().words != 0 && ix.view().words != a.ix.words)
+        throw std::runtime_error("SEISMIC lists and forward index disagree on the dimension");
     a.q.n = n;
     a.q.indptr = d_indptr;
     a.q.idx = d_idx;

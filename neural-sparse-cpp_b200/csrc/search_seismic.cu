@@ -681,6 +681,18 @@ size_t seismic_smem_per_warp(int val_kind, int dim_words, int qcap, int k) {
 int seismic_max_blocks_per_sm(int val_kind, int warps_per_block, size_t smem) {
     int blocks = 0;
     cudaError_t e = cudaSuccess;
+    // the occupancy calculator only admits dynamic shared memory the kernel
+    // has been allowed to use
+    if (val_kind == kF32)
+        e = cudaFuncSetAttribute(seismic_search_kernel<float>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    else if (val_kind == kU8)
+        e = cudaFuncSetAttribute(seismic_search_kernel<uint8_t>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    else
+        e = cudaFuncSetAttribute(seismic_search_kernel<uint16_t>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return 0;
     if (val_kind == kF32)
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, seismic_search_kernel<float>,
                                                           warps_per_block * 32, smem);
