@@ -1,0 +1,373 @@
+"""Benchmark: SEISMIC FP32 search at 1M docs (the reference's shape: SPLADE
+vectors over the 30,522-term BERT vocabulary), queries per second.
+
+Workload (synthetic, seeded; stands in for MS MARCO SPLADE): 1,000,000 docs
+with lognormal nnz (median 110, clipped 10-400), 10,000 queries (median 25,
+clipped 3-120), Zipf(1.1) terms without replacement, lognormal(0, 0.8) values.
+Index: seismic, lambda=4000 (posting cap), beta=400 (blocks per list =
+0.1 * lambda), alpha=0.4, seed=7, built on the GPU. Search: cut=10,
+heap_factor=0.8, k=10.
+
+A step is one batched search of the 10,000 queries (one persistent kernel
+launch). `value` times the device-resident call (queries and results in HBM);
+`e2e` times the host-buffer call (the reference-facing API: pinned H2D of the
+queries, search, D2H of the results). The index (~5 GB) exceeds L2, and L2 is
+also flushed between timed steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun each rank is a replica holding the whole index and searching
+its own 10,000 queries (weak scaling, no collective on the data path).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (os.path.join(ROOT, "neural-sparse-cpp_b200", "python"), os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+N_DOCS = 1_000_000
+N_QUERIES = 10_000
+SPEC = "seismic,lambda=4000|beta=400|alpha=0.4|seed=7"
+CUT, HF, K = 10, 0.8, 10
+METRIC = "QPS@recall@10 (SEISMIC fp32, batched, 1M docs)"
+WORKLOAD = {"workload": "seismic_fp32_1M_docs_10k_queries", "docs": N_DOCS, "queries": N_QUERIES,
+            "vocab": 30522, "lambda": 4000, "beta": 400, "alpha": 0.4, "cut": CUT,
+            "heap_factor": HF, "k": K, "l2": "flushed between steps; index > L2"}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    QUERY = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 3 + i and r[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(self.rows)}
+
+
+def make_data(rank):
+    from nsparse_b200 import synth
+    docs = synth.docs_config0(N_DOCS, seed=0)
+    qs = synth.queries_config0(N_QUERIES, seed=1000 + rank)
+    return docs, qs
+
+
+def recall_at_k(L, T):
+    v = []
+    for a, b in zip(L, T):
+        want = set(int(x) for x in b if x >= 0)
+        if want:
+            v.append(len(set(int(x) for x in a if x >= 0) & want) / len(want))
+    return float(np.mean(v)) if v else 1.0
+
+
+def cpu_baseline(docs, qs, index_file, sample):
+    """The reference's own search (compiled from its sources, oracle/_ref), all
+    host threads, on the first `sample` queries of the workload."""
+    import oracle as O
+    variant = ref_variant()
+    if variant is None:
+        return None
+    L = O.ref_lib(variant)
+    cores = os.cpu_count()
+    L.ref_set_threads(cores)
+    r = O.RefIndex.read(index_file, variant=variant)
+    q = qs.rows(0, sample)
+    r.search(q.rows(0, min(64, sample)), K, param_kind=2, cut=CUT, heap_factor=HF)  # warm
+    t = time.perf_counter()
+    r.search(q, K, param_kind=2, cut=CUT, heap_factor=HF)
+    dt = time.perf_counter() - t
+    r.close()
+    return {"value": sample / dt, "unit": "queries/s", "cores": cores, "kind": "reference",
+            "sample": f"{sample} of the {N_QUERIES} queries, one batched search() call, "
+                      f"reference {variant} build, OMP threads={cores}"}
+
+
+def ref_variant():
+    import oracle as O
+    flags = open("/proc/cpuinfo").read()
+    for v, need in (("avx512", "avx512bw"), ("avx2", "avx2"), ("generic", "")):
+        if O.ref_available(v) and (not need or need in flags):
+            return v
+    return None
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle as O
+    variant = ref_variant()
+    if variant is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference library not built (oracle/_ref)"}))
+        return
+    docs, qs = make_data(0)
+    cores = os.cpu_count()
+    O.ref_lib(variant).ref_set_threads(cores)
+    t = time.perf_counter()
+    r = O.RefIndex(docs.dim, SPEC, variant=variant)
+    r.add(docs)
+    r.build()
+    build_s = time.perf_counter() - t
+    log(f"reference build {build_s:.1f}s on {cores} threads")
+    sample = 2000  # queries per step: ~10-30 s of CPU work
+    q = qs.rows(0, sample)
+    for _ in range(args.warmup):
+        r.search(q.rows(0, 200), K, param_kind=2, cut=CUT, heap_factor=HF)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        r.search(q, K, param_kind=2, cut=CUT, heap_factor=HF)
+        times.append(time.perf_counter() - t)
+    value = sample * len(times) / sum(times)
+    out = {"metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": 0, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1000 * sum(times) / len(times),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic", "impl": "reference", "config": dict(WORKLOAD, sample_queries=sample),
+           "build_s": build_s,
+           "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cores, "kind": "reference",
+                            "sample": f"{sample} queries per step, one batched search() call, "
+                                      f"reference {variant} build"},
+           "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def run_engine(args):
+    import torch
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    import nsparse
+    dev = torch.device("cuda", torch.cuda.current_device())
+    docs, qs = make_data(rank)
+
+    # ---- build on the GPU
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    idx = nsparse.index_factory(docs.dim, SPEC)
+    idx.add(docs.n, docs.indptr, docs.indices, docs.values)
+    idx.build()
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t
+    log(f"rank {rank}: device build {build_s:.1f}s")
+    params = nsparse.SeismicSearchParameters(CUT, HF)
+
+    # ---- device-resident inputs and outputs
+    d_ip = torch.from_numpy(qs.indptr).to(dev)
+    d_ix = torch.from_numpy(qs.indices.view(np.int16)).to(dev)
+    d_v = torch.from_numpy(qs.values).to(dev)
+    d_D = torch.empty((qs.n, K), dtype=torch.float32, device=dev)
+    d_L = torch.empty((qs.n, K), dtype=torch.int32, device=dev)
+    max_nnz = int(np.diff(qs.indptr).max())
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+
+    def step():
+        idx.search_device(qs.n, d_ip.data_ptr(), d_ix.data_ptr(), d_v.data_ptr(), max_nnz, K,
+                          d_D.data_ptr(), d_L.data_ptr(), params, stream.cuda_stream)
+
+    idx.search(qs.n, qs.indptr, qs.indices, qs.values, K, params)  # uploads lists
+    for _ in range(max(args.warmup, 3)):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with Clocks(torch.cuda.current_device()) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    # kernel-only time and algorithmic bytes of one batched search (engine stats)
+    D, L = idx.search(qs.n, qs.indptr, qs.indices, qs.values, K, params)
+    st = nsparse.last_search_stats()
+    hD, hL = d_D.cpu().numpy(), d_L.cpu().numpy()
+    assert (hL == L).all() and (hD == D).all(), "device-resident and host paths disagree"
+
+    # ---- e2e: host buffers through the public API, copies included
+    e2e_t = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        idx.search(qs.n, qs.indptr, qs.indices, qs.values, K, params)
+        e2e_t.append(time.perf_counter() - t)
+    h2d = 4 * (qs.n + 1) + 2 * qs.nnz + 4 * qs.nnz
+    d2h = qs.n * K * 8
+
+    # ---- plain per-query path on a sample, and recall vs exact
+    plain = nsparse.SeismicSearchParameters(CUT, HF)
+    plain.set_engine(plain=True)
+    n_plain = 300
+    qp = qs.rows(0, n_plain)
+    idx.search(qp.rows(0, 4).n, qp.rows(0, 4).indptr, qp.rows(0, 4).indices, qp.rows(0, 4).values,
+               K, plain)
+    lat = []
+    for q in range(n_plain):
+        r1 = qp.rows(q, q + 1)
+        t = time.perf_counter()
+        Dp, Lp = idx.search(1, r1.indptr, r1.indices, r1.values, K, plain)
+        lat.append(time.perf_counter() - t)
+        assert (Lp[0] == L[q]).all()
+    plain_qps = n_plain / sum(lat)
+    brute = nsparse.index_factory(docs.dim, "inverted")
+    brute.add(docs.n, docs.indptr, docs.indices, docs.values)
+    brute.build()
+    _, Lt = brute.search(qs.n, qs.indptr, qs.indices, qs.values, K)
+    rec = recall_at_k(L, Lt)
+    del brute
+
+    # ---- aggregate over ranks: max time
+    my_ms = total_ms
+    if world > 1:
+        t_ = torch.tensor([my_ms], device=dev)
+        torch.distributed.all_reduce(t_, op=torch.distributed.ReduceOp.MAX)
+        my_ms = float(t_.item())
+    value = world * qs.n * args.steps / (my_ms / 1000.0)
+    e2e_value = world * qs.n * len(e2e_t) / sum(e2e_t)
+    if world > 1:
+        t_ = torch.tensor([sum(e2e_t)], device=dev)
+        torch.distributed.all_reduce(t_, op=torch.distributed.ReduceOp.MAX)
+        e2e_value = world * qs.n * len(e2e_t) / float(t_.item())
+
+    peak, peak_kind = measured_peaks()
+    achieved = st.bytes / (st.kernel_ms / 1000.0) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "seismic_search_fp32_1M.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            with tempfile.TemporaryDirectory() as td:
+                fpath = os.path.join(td, "c1.idx")
+                nsparse.write_index(idx, fpath)
+                cpu = cpu_baseline(docs, qs, fpath, 2000)
+        lat_ms = sorted(1000 * x for x in lat)
+        out = {
+            "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": my_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": dict(WORKLOAD, parallelism=f"replicas{world}"),
+            "recall_at_10": rec, "build_s": build_s,
+            "plain": {"qps": plain_qps, "queries": n_plain,
+                      "p50_ms": lat_ms[len(lat_ms) // 2], "p99_ms": lat_ms[int(0.99 * (len(lat_ms) - 1))],
+                      "batched_over_plain": value / world / plain_qps},
+            "batch_latency_ms": {"p50": statistics.median(step_ms), "max": max(step_ms)},
+            "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": st.bytes,
+                         "kernel_ms_per_launch": st.kernel_ms},
+            "work": {"docs_scored_per_query": st.docs_scored / qs.n,
+                     "blocks_visited_per_query": st.blocks_visited / qs.n},
+            "gpu_launches": args.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out))
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_engine(args)
+
+
+if __name__ == "__main__":
+    main()

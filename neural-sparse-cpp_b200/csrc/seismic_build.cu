@@ -1,13 +1,904 @@
-// SEISMIC index build on the device.
-#include <stdexcept>
+// SEISMIC index build on the device (the reference's
+// build_inverted_lists_clusters, seismic_common.h:146-184).
+//
+//  1. postings      one warp per document scatters its (term, doc, value)
+//                   entries into per-term lists (warp-aggregated atomics);
+//                   a segmented sort orders each list: by value descending,
+//                   then doc ascending, when it exceeds the posting cap lambda
+//                   (invlists/inverted_lists.cpp:110-132), else by doc
+//                   (the order build_inverted_lists produces, :159-180).
+//  2. centroids     drawn on the host with std::mt19937 and
+//                   std::uniform_int_distribution<> seeded base_seed + list,
+//                   the reference's own draw (cluster/random_kmeans.cpp:28-51);
+//                   it depends only on list lengths, so only those come back.
+//  3. assignment    one CTA per list: the centroids' terms are indexed term
+//                   major in scratch, one warp per document accumulates its
+//                   similarity to every centroid in the document's term order
+//                   (cluster/kmeans_utils.cpp:131-145; fp32 products and sums
+//                   rounded separately, int64 for codes) and takes the strict
+//                   argmax, lowest index on ties (:147-156).
+//  4. blocks        a stable segmented sort puts each centroid first and its
+//                   members after it in list order.
+//  5. summaries     per block: entries sorted by term (stable), a per-term
+//                   running max gives each entry's increment of the block's
+//                   mass, summed in the reference's entry order
+//                   (cluster/inverted_list_clusters.cpp:72-124); the maxima
+//                   are sorted by value descending (term ascending on ties)
+//                   and cut where the running mass reaches alpha (:37-65),
+//                   then transposed term-major per list (:230-293).
+// The lists come back to the host for persistence and are uploaded in the
+// search layout.
+#include <cub/device/device_segmented_sort.cuh>
+#include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <random>
+#include <stdexcept>
+#include <thread>
+#include <vector>
+
+#include "engine.h"
 #include "index_state.h"
+#include "scan.h"
 
 namespace nsparse {
 namespace detail {
+namespace {
 
-void seismic_build(SeismicState&, int, const SeismicClusterParameters&) {
-    throw std::runtime_error("SEISMIC device build is not available in this build");
+using nsp::cuda_check;
+using nsp::DevArray;
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// ------------------------------------------------------- parameters ------
+
+// seismic_common.h:130-144
+int calc_lambda(int lambda, size_t n_vectors) {
+    if (lambda == -1)
+        return std::max(static_cast<int>(0.0005F * static_cast<float>(n_vectors)), 160);
+    return lambda;
+}
+
+int calc_beta(int beta, int lambda) {
+    if (beta == -1) return static_cast<int>(static_cast<float>(lambda) * 0.1F);
+    return beta;
+}
+
+// random_kmeans.cpp:53-63 with the caller's int beta converted to size_t.
+size_t clusters_for(size_t n_docs, int beta) {
+    size_t nc = static_cast<size_t>(static_cast<long long>(beta));  // wraps like the reference
+    if (beta == 0) nc = static_cast<size_t>(std::sqrt(n_docs));
+    nc = nc > n_docs ? n_docs : nc;
+    return std::max<size_t>(1, nc);
+}
+
+// Positions (into the list's kept order) of the centroids of one list:
+// random_kmeans.cpp:28-51, applied to positions instead of ids.
+void draw_positions(size_t n, size_t nc, uint32_t seed, std::vector<int32_t>& perm,
+                    int32_t* out) {
+    perm.resize(n);
+    for (size_t i = 0; i < n; ++i) perm[i] = static_cast<int32_t>(i);
+    std::mt19937 gen(seed);
+    for (size_t i = 0; i < nc; ++i) {
+        std::uniform_int_distribution<> distrib(0, static_cast<int>(n - i - 1));
+        const size_t r = static_cast<size_t>(distrib(gen));
+        out[i] = perm[r];
+        std::swap(perm[r], perm[n - 1 - i]);
+    }
+}
+
+// ------------------------------------------------------------- keys ------
+
+// Order-preserving map of a value to uint32 (ascending value = ascending key).
+__device__ __forceinline__ uint32_t orderable(float v) {
+    const uint32_t b = __float_as_uint(v);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+template <int ESZ>
+__device__ __forceinline__ float value_at(const uint8_t* val, int64_t i) {
+    if constexpr (ESZ == 4) return reinterpret_cast<const float*>(val)[i];
+    if constexpr (ESZ == 2) return static_cast<float>(reinterpret_cast<const uint16_t*>(val)[i]);
+    return static_cast<float>(val[i]);
+}
+
+// ------------------------------------------------------------ 1. postings --
+
+__global__ void post_count_kernel(nsp::FwdView f, unsigned long long* cnt) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t d = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
+         d < f.n_docs; d += warps) {
+        const uint2 ri = f.rowinfo[d];
+        const uint16_t* ip = f.idx + static_cast<size_t>(ri.x) * nsp::kRowAlign;
+        for (uint32_t e0 = 0; e0 < ri.y; e0 += 32) {
+            const uint32_t e = e0 + lane;
+            const bool valid = e < ri.y;
+            const uint32_t t = valid ? ip[e] : 0xffffffffu;
+            const unsigned peers = __match_any_sync(kFull, t);
+            if (valid && (__ffs(peers) - 1) == lane) atomicAdd(cnt + t, __popc(peers));
+        }
+    }
+}
+
+// Writes each entry's sort key into its list: (~value << 32 | doc) when the
+// list is over the cap, doc otherwise.
+template <int ESZ>
+__global__ void post_scatter_kernel(nsp::FwdView f, const int64_t* post_ptr,
+                                    unsigned long long* cursor, int64_t cap,
+                                    uint64_t* keys) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+    const uint8_t* vals = static_cast<const uint8_t*>(f.val);
+    for (int64_t d = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
+         d < f.n_docs; d += warps) {
+        const uint2 ri = f.rowinfo[d];
+        const int64_t base = static_cast<int64_t>(ri.x) * nsp::kRowAlign;
+        for (uint32_t e0 = 0; e0 < ri.y; e0 += 32) {
+            const uint32_t e = e0 + lane;
+            const bool valid = e < ri.y;
+            const uint32_t t = valid ? f.idx[base + e] : 0xffffffffu;
+            const unsigned peers = __match_any_sync(kFull, t);
+            const int leader = __ffs(peers) - 1;
+            unsigned long long start = 0;
+            if (valid && leader == lane) start = atomicAdd(cursor + t, __popc(peers));
+            start = __shfl_sync(kFull, start, leader);
+            if (valid) {
+                const int rank = __popc(peers & ((1u << lane) - 1u));
+                const int64_t len = post_ptr[t + 1] - post_ptr[t];
+                const uint64_t key =
+                    (cap > 0 && len > cap)
+                        ? (static_cast<uint64_t>(~orderable(value_at<ESZ>(vals, base + e))) << 32) |
+                              static_cast<uint32_t>(d)
+                        : static_cast<uint64_t>(static_cast<uint32_t>(d));
+                keys[post_ptr[t] + static_cast<int64_t>(start) + rank] = key;
+            }
+        }
+    }
+}
+
+__global__ void kept_copy_kernel(const uint64_t* keys, const int64_t* post_ptr,
+                                 const int64_t* kept_ptr, int32_t n_lists, int32_t* kept) {
+    for (int32_t t = blockIdx.x; t < n_lists; t += gridDim.x) {
+        const int64_t n = kept_ptr[t + 1] - kept_ptr[t];
+        for (int64_t i = threadIdx.x; i < n; i += blockDim.x)
+            kept[kept_ptr[t] + i] = static_cast<int32_t>(keys[post_ptr[t] + i] & 0xffffffffu);
+    }
+}
+
+// ---------------------------------------------------------- 3. assignment --
+
+struct AssignArgs {
+    nsp::FwdView f;
+    int32_t n_lists;
+    const int64_t* kept_ptr;
+    const int32_t* kept;
+    const int64_t* cptr;
+    const int32_t* cpos;
+    uint32_t* out_key;      // per kept position: cluster * 2 + (centroid ? 0 : 1)
+    int32_t* work;          // list counter
+    // per-CTA scratch
+    int32_t* tcnt;          // [dim] per CTA, zero between lists
+    int32_t* tstart;        // [dim] per CTA
+    int32_t* tcur;          // [dim] per CTA
+    int32_t* touched;       // [max centroid entries] per CTA
+    uint16_t* ccl;          // [max centroid entries] per CTA
+    uint8_t* cw;            // [max centroid entries * esz] per CTA
+    uint8_t* is_centroid;   // [max kept] per CTA
+    void* sims;             // per warp [max nc] (float or int64)
+    int64_t max_centroid_entries;
+    int64_t max_kept;
+    int32_t max_nc;
+};
+
+template <int ESZ>
+__global__ void __launch_bounds__(256) assign_kernel(AssignArgs a) {
+    using acc_t = typename std::conditional<ESZ == 4, float, long long>::type;
+    __shared__ int32_t s_list;
+    __shared__ int32_t s_touched;
+    __shared__ int32_t s_total;
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    const int dim = a.f.dim;
+    int32_t* tcnt = a.tcnt + static_cast<size_t>(blockIdx.x) * dim;
+    int32_t* tstart = a.tstart + static_cast<size_t>(blockIdx.x) * dim;
+    int32_t* tcur = a.tcur + static_cast<size_t>(blockIdx.x) * dim;
+    int32_t* touched = a.touched + static_cast<size_t>(blockIdx.x) * a.max_centroid_entries;
+    uint16_t* ccl = a.ccl + static_cast<size_t>(blockIdx.x) * a.max_centroid_entries;
+    uint8_t* cw = a.cw + static_cast<size_t>(blockIdx.x) * a.max_centroid_entries * ESZ;
+    uint8_t* isc = a.is_centroid + static_cast<size_t>(blockIdx.x) * a.max_kept;
+    acc_t* sims = static_cast<acc_t*>(a.sims) +
+                  static_cast<size_t>(blockIdx.x * wpb + warp) * a.max_nc;
+    const uint8_t* fval = static_cast<const uint8_t*>(a.f.val);
+
+    for (;;) {
+        if (threadIdx.x == 0) s_list = atomicAdd(a.work, 1);
+        __syncthreads();
+        const int32_t t = s_list;
+        __syncthreads();
+        if (t >= a.n_lists) break;
+        const int64_t kb = a.kept_ptr[t];
+        const int32_t n = static_cast<int32_t>(a.kept_ptr[t + 1] - kb);
+        const int32_t nc = static_cast<int32_t>(a.cptr[t + 1] - a.cptr[t]);
+        if (n == 0) continue;
+        const int32_t* cp = a.cpos + a.cptr[t];
+        for (int32_t i = threadIdx.x; i < n; i += blockDim.x) isc[i] = 0;
+        if (threadIdx.x == 0) {
+            s_touched = 0;
+            s_total = 0;
+        }
+        __syncthreads();
+        for (int32_t c = threadIdx.x; c < nc; c += blockDim.x) isc[cp[c]] = 1;
+        // index the centroid entries by term: count, ranges, scatter
+        for (int32_t c = warp; c < nc; c += wpb) {
+            const int32_t doc = a.kept[kb + cp[c]];
+            const uint2 ri = a.f.rowinfo[doc];
+            const uint16_t* ip = a.f.idx + static_cast<size_t>(ri.x) * nsp::kRowAlign;
+            for (uint32_t e = lane; e < ri.y; e += 32) {
+                const int32_t term = ip[e];
+                if (atomicAdd(tcnt + term, 1) == 0) touched[atomicAdd(&s_touched, 1)] = term;
+            }
+        }
+        __syncthreads();
+        const int32_t nt = s_touched;
+        for (int32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+            const int32_t term = touched[i];
+            tstart[term] = atomicAdd(&s_total, tcnt[term]);
+            tcur[term] = 0;
+        }
+        __syncthreads();
+        for (int32_t c = warp; c < nc; c += wpb) {
+            const int32_t doc = a.kept[kb + cp[c]];
+            const uint2 ri = a.f.rowinfo[doc];
+            const int64_t rb = static_cast<int64_t>(ri.x) * nsp::kRowAlign;
+            for (uint32_t e = lane; e < ri.y; e += 32) {
+                const int32_t term = a.f.idx[rb + e];
+                const int32_t pos = tstart[term] + atomicAdd(tcur + term, 1);
+                ccl[pos] = static_cast<uint16_t>(c);
+                for (int b = 0; b < ESZ; ++b) cw[static_cast<size_t>(pos) * ESZ + b] = fval[(rb + e) * ESZ + b];
+            }
+        }
+        __syncthreads();
+        // assign every non-centroid doc, one warp per doc
+        for (int32_t p = warp; p < n; p += wpb) {
+            if (isc[p]) {
+                // centroid: its own cluster, placed first
+                if (lane == 0) {
+                    int32_t c = 0;
+                    while (cp[c] != p) ++c;
+                    a.out_key[kb + p] = static_cast<uint32_t>(c) * 2u;
+                }
+                continue;
+            }
+            const int32_t doc = a.kept[kb + p];
+            for (int32_t c = lane; c < nc; c += 32) sims[c] = 0;
+            __syncwarp();
+            const uint2 ri = a.f.rowinfo[doc];
+            const int64_t rb = static_cast<int64_t>(ri.x) * nsp::kRowAlign;
+            for (uint32_t e0 = 0; e0 < ri.y; e0 += 32) {
+                const uint32_t e = e0 + lane;
+                int32_t rs = 0, rn = 0;
+                acc_t v = 0;
+                if (e < ri.y) {
+                    const int32_t term = a.f.idx[rb + e];
+                    rn = tcnt[term];
+                    if (rn > 0) rs = tstart[term];
+                    if constexpr (ESZ == 4) v = reinterpret_cast<const float*>(fval)[rb + e];
+                    else if constexpr (ESZ == 2) v = reinterpret_cast<const uint16_t*>(fval)[rb + e];
+                    else v = fval[rb + e];
+                }
+                // doc terms in order (kmeans_utils.cpp:134-145)
+                unsigned m = __ballot_sync(kFull, rn > 0);
+                while (m) {
+                    const int src = __ffs(m) - 1;
+                    m &= m - 1;
+                    const int32_t s0 = __shfl_sync(kFull, rs, src);
+                    const int32_t cnt = __shfl_sync(kFull, rn, src);
+                    const acc_t dv = __shfl_sync(kFull, v, src);
+                    for (int32_t k = lane; k < cnt; k += 32) {
+                        const int32_t c = ccl[s0 + k];
+                        if constexpr (ESZ == 4) {
+                            const float w = reinterpret_cast<const float*>(cw)[s0 + k];
+                            sims[c] = __fadd_rn(sims[c], __fmul_rn(dv, w));
+                        } else if constexpr (ESZ == 2) {
+                            sims[c] += dv * static_cast<long long>(reinterpret_cast<const uint16_t*>(cw)[s0 + k]);
+                        } else {
+                            sims[c] += dv * static_cast<long long>(cw[s0 + k]);
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+            // strict >, ascending: ties go to the lowest cluster (kmeans_utils.cpp:147-156)
+            acc_t best = 0;
+            int32_t bi = -1;
+            for (int32_t c = lane; c < nc; c += 32) {
+                const acc_t s = sims[c];
+                if (bi < 0 || s > best) {
+                    best = s;
+                    bi = c;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const acc_t s2 = __shfl_xor_sync(kFull, best, o);
+                const int32_t i2 = __shfl_xor_sync(kFull, bi, o);
+                if (i2 >= 0 && (bi < 0 || s2 > best || (s2 == best && i2 < bi))) {
+                    best = s2;
+                    bi = i2;
+                }
+            }
+            if (lane == 0) a.out_key[kb + p] = static_cast<uint32_t>(bi) * 2u + 1u;
+            __syncwarp();
+        }
+        __syncthreads();
+        for (int32_t i = threadIdx.x; i < nt; i += blockDim.x) tcnt[touched[i]] = 0;
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------ 5. summaries --
+
+// Entries of a batch of blocks: for block b (global id), its docs' rows in
+// block order. term -> ekey, value -> eval, original index -> eidx.
+template <int ESZ>
+__global__ void entries_kernel(nsp::FwdView f, const int32_t* docs, const int64_t* bdp,
+                               int64_t b0, int64_t nb, const int64_t* doc_eoff, int64_t e_base,
+                               uint16_t* ekey, uint32_t* eidx, float* eval) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+    const int64_t d0 = bdp[b0], d1 = bdp[b0 + nb];
+    const uint8_t* vals = static_cast<const uint8_t*>(f.val);
+    for (int64_t j = d0 + ((blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5); j < d1;
+         j += warps) {
+        const int32_t doc = docs[j];
+        const uint2 ri = f.rowinfo[doc];
+        const int64_t rb = static_cast<int64_t>(ri.x) * nsp::kRowAlign;
+        const int64_t out = doc_eoff[j - d0] - e_base;
+        for (uint32_t e = lane; e < ri.y; e += 32) {
+            ekey[out + e] = f.idx[rb + e];
+            eidx[out + e] = static_cast<uint32_t>(out + e);
+            eval[out + e] = value_at<ESZ>(vals, rb + e);
+        }
+    }
+}
+
+// One thread per (block, term) run of the term-sorted entries: the running max
+// gives each entry's increment of the block mass (inverted_list_clusters.cpp:
+// 96-114); the run's final max becomes a candidate summary pair.
+template <int ESZ>
+__global__ void runs_kernel(const uint16_t* skey, const uint32_t* sidx, const float* eval,
+                            const int32_t* run_start, int64_t n_runs, int64_t n_entries,
+                            const int32_t* entry_block, float* delta, uint8_t* has_delta,
+                            uint64_t* pkey, int32_t* pblock) {
+    for (int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; r < n_runs;
+         r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t s = run_start[r];
+        const int64_t e = r + 1 < n_runs ? run_start[r + 1] : n_entries;
+        float acc = 0.0f;
+        for (int64_t i = s; i < e; ++i) {
+            const uint32_t oi = sidx[i];
+            const float v = eval[oi];
+            if (i == s) {
+                // first touch: max(T(0), v)
+                acc = v > 0.0f ? v : 0.0f;
+                delta[oi] = acc;
+                has_delta[oi] = 1;
+            } else if (v > acc) {
+                if constexpr (ESZ == 4) delta[oi] = __fsub_rn(v, acc);
+                else delta[oi] = static_cast<float>(static_cast<int>(v) - static_cast<int>(acc));
+                has_delta[oi] = 1;
+                acc = v;
+            } else {
+                has_delta[oi] = 0;
+            }
+        }
+        const uint32_t term = skey[s];
+        // sort key for the alpha cut: value descending, term ascending
+        pkey[r] = (static_cast<uint64_t>(~orderable(acc)) << 16) | term;
+        pblock[r] = entry_block[sidx[s]];
+    }
+}
+
+__device__ __forceinline__ float unorderable(uint32_t k) {
+    const uint32_t b = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+    return __uint_as_float(b);
+}
+
+// alpha cut (inverted_list_clusters.cpp:43-51): one thread per block walks its
+// pairs by value descending, summing until addup / sum >= alpha.
+__global__ void cut_kernel(const uint64_t* pkey_sorted, const int64_t* pair_off, int64_t nb,
+                           const float* mass, float alpha, int32_t* keep) {
+    for (int64_t b = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; b < nb;
+         b += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t s = pair_off[b], e = pair_off[b + 1];
+        float addup = 0.0f;
+        int32_t k = static_cast<int32_t>(e - s);
+        for (int64_t i = s; i < e; ++i) {
+            const float v = unorderable(~static_cast<uint32_t>(pkey_sorted[i] >> 16));
+            addup = __fadd_rn(addup, v);
+            if (__fdiv_rn(addup, mass[b]) >= alpha) {
+                k = static_cast<int32_t>(i - s + 1);
+                break;
+            }
+        }
+        keep[b] = k;
+    }
+}
+
+template <class K, class V>
+void segmented_sort_pairs(const K* kin, K* kout, const V* vin, V* vout, int64_t n,
+                          int64_t segs, const int32_t* off, cudaStream_t s, bool stable) {
+    if (n == 0 || segs == 0) return;
+    if (n > INT32_MAX || segs > INT32_MAX) throw std::invalid_argument("build batch too large");
+    size_t tmp = 0;
+    if (stable)
+        cuda_check(cub::DeviceSegmentedSort::StableSortPairs(nullptr, tmp, kin, kout, vin, vout,
+                                                             static_cast<int>(n), static_cast<int>(segs),
+                                                             off, off + 1, s), "cub sort");
+    else
+        cuda_check(cub::DeviceSegmentedSort::SortPairs(nullptr, tmp, kin, kout, vin, vout,
+                                                       static_cast<int>(n), static_cast<int>(segs),
+                                                       off, off + 1, s), "cub sort");
+    DevArray<uint8_t> t(tmp + 16);
+    if (stable)
+        cuda_check(cub::DeviceSegmentedSort::StableSortPairs(t.data(), tmp, kin, kout, vin, vout,
+                                                             static_cast<int>(n), static_cast<int>(segs),
+                                                             off, off + 1, s), "cub sort");
+    else
+        cuda_check(cub::DeviceSegmentedSort::SortPairs(t.data(), tmp, kin, kout, vin, vout,
+                                                       static_cast<int>(n), static_cast<int>(segs),
+                                                       off, off + 1, s), "cub sort");
+    cuda_check(cudaStreamSynchronize(s), "sort sync");
+}
+
+template <class K>
+void segmented_sort_keys(const K* kin, K* kout, int64_t n, int64_t segs, const int32_t* off,
+                         cudaStream_t s) {
+    if (n == 0 || segs == 0) return;
+    if (n > INT32_MAX || segs > INT32_MAX) throw std::invalid_argument("build batch too large");
+    size_t tmp = 0;
+    cuda_check(cub::DeviceSegmentedSort::SortKeys(nullptr, tmp, kin, kout, static_cast<int>(n),
+                                                  static_cast<int>(segs), off, off + 1, s),
+               "cub sort");
+    DevArray<uint8_t> t(tmp + 16);
+    cuda_check(cub::DeviceSegmentedSort::SortKeys(t.data(), tmp, kin, kout, static_cast<int>(n),
+                                                  static_cast<int>(segs), off, off + 1, s),
+               "cub sort");
+    cuda_check(cudaStreamSynchronize(s), "sort sync");
+}
+
+template <class T>
+std::vector<T> to_host(const DevArray<T>& d, size_t n, cudaStream_t s) {
+    std::vector<T> h(n);
+    d.download(h.data(), n, s);
+    cuda_check(cudaStreamSynchronize(s), "D2H");
+    return h;
+}
+
+template <class T>
+void to_dev(DevArray<T>& d, const std::vector<T>& h, cudaStream_t s) {
+    d.upload(h.data(), h.size(), s);
+}
+
+std::vector<int32_t> to_i32_offsets(const std::vector<int64_t>& v) {
+    std::vector<int32_t> o(v.size());
+    for (size_t i = 0; i < v.size(); ++i) {
+        if (v[i] > INT32_MAX) throw std::invalid_argument("build batch too large");
+        o[i] = static_cast<int32_t>(v[i]);
+    }
+    return o;
+}
+
+__global__ void fill_block_kernel(const int32_t* boff, int64_t nb, int32_t* entry_block) {
+    for (int64_t b = blockIdx.x; b < nb; b += gridDim.x)
+        for (int64_t i = boff[b] + threadIdx.x; i < boff[b + 1]; i += blockDim.x)
+            entry_block[i] = static_cast<int32_t>(b);
+}
+
+// 1 where a (block, term) run starts in the term-sorted entries.
+__global__ void run_flag_kernel(const uint16_t* skey, const int32_t* entry_block, int64_t ne,
+                                int64_t* flag) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < ne;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        flag[i] = (i == 0 || entry_block[i] != entry_block[i - 1] || skey[i] != skey[i - 1]) ? 1 : 0;
+}
+
+__global__ void run_compact_kernel(const int64_t* flag, const int64_t* pos, int64_t ne,
+                                   int32_t* run_start) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < ne;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        if (flag[i]) run_start[pos[i]] = static_cast<int32_t>(i);
+}
+
+__global__ void mass_kernel(const float* delta, const uint8_t* has_delta, const int32_t* boff,
+                            int64_t nb, float* mass) {
+    for (int64_t b = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; b < nb;
+         b += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        float sum = 0.0f;
+        for (int64_t i = boff[b]; i < boff[b + 1]; ++i)
+            if (has_delta[i]) sum = __fadd_rn(sum, delta[i]);
+        mass[b] = sum;
+    }
+}
+
+// Kept pairs of each block, keyed (term << 16 | block within its list) for
+// the per-list term-major transpose.
+__global__ void kept_pairs_kernel(const uint64_t* pkey_sorted, const int64_t* pair_off,
+                                  const int32_t* keep, const int64_t* kept_off,
+                                  const uint16_t* block_local, int64_t nb, uint32_t* tkey,
+                                  float* tval) {
+    for (int64_t b = blockIdx.x; b < nb; b += gridDim.x) {
+        for (int32_t i = threadIdx.x; i < keep[b]; i += blockDim.x) {
+            const uint64_t k = pkey_sorted[pair_off[b] + i];
+            const uint32_t term = static_cast<uint32_t>(k & 0xffffu);
+            tkey[kept_off[b] + i] = (term << 16) | block_local[b];
+            tval[kept_off[b] + i] = unorderable(~static_cast<uint32_t>(k >> 16));
+        }
+    }
+}
+
+template <int ESZ>
+void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
+                     const DevArray<int64_t>& d_bdp, nsp::SeismicHost& L, int32_t t0, int32_t t1,
+                     const std::vector<int64_t>& doc_eoff, const std::vector<int64_t>& blk_e,
+                     float alpha, cudaStream_t s) {
+    const int sms = nsp::device_sm_count();
+    const int64_t b0 = L.lbp[t0], b1 = L.lbp[t1];
+    const int64_t nb = b1 - b0;
+    const int64_t e0 = blk_e[b0], ne = blk_e[b1] - e0;
+    // entries in block order
+    std::vector<int64_t> bdoc_eoff(doc_eoff.begin() + L.bdp[b0], doc_eoff.begin() + L.bdp[b1] + 1);
+    DevArray<int64_t> d_doc_eoff;
+    to_dev(d_doc_eoff, bdoc_eoff, s);
+    DevArray<uint16_t> ekey(ne), skey(ne);
+    DevArray<uint32_t> eidx(ne), sidx(ne);
+    DevArray<float> eval(ne);
+    entries_kernel<ESZ><<<sms * 8, 256, 0, s>>>(f, d_docs.data(), d_bdp.data(), b0, nb,
+                                                d_doc_eoff.data(), e0, ekey.data(), eidx.data(),
+                                                eval.data());
+    cuda_check(cudaGetLastError(), "entries_kernel");
+    std::vector<int64_t> boff64(blk_e.begin() + b0, blk_e.begin() + b1 + 1);
+    for (auto& v : boff64) v -= e0;
+    DevArray<int32_t> d_boff;
+    to_dev(d_boff, to_i32_offsets(boff64), s);
+    // stable: entries of a term stay in block order
+    segmented_sort_pairs(ekey.data(), skey.data(), eidx.data(), sidx.data(), ne, nb,
+                         d_boff.data(), s, /*stable=*/true);
+    ekey.reset();
+    eidx.reset();
+    DevArray<int32_t> entry_block(ne);
+    fill_block_kernel<<<sms * 8, 256, 0, s>>>(d_boff.data(), nb, entry_block.data());
+    cuda_check(cudaGetLastError(), "fill_block_kernel");
+    DevArray<int64_t> flag(ne), pos(ne);
+    run_flag_kernel<<<sms * 8, 256, 0, s>>>(skey.data(), entry_block.data(), ne, flag.data());
+    cuda_check(cudaGetLastError(), "run_flag_kernel");
+    nsp::exclusive_scan_i64(flag.data(), pos.data(), ne, s);
+    int64_t last_pos = 0, last_flag = 0;
+    cuda_check(cudaMemcpyAsync(&last_pos, pos.data() + ne - 1, 8, cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaMemcpyAsync(&last_flag, flag.data() + ne - 1, 8, cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    const int64_t n_runs = last_pos + last_flag;
+    DevArray<int32_t> run_start(n_runs);
+    run_compact_kernel<<<sms * 8, 256, 0, s>>>(flag.data(), pos.data(), ne, run_start.data());
+    cuda_check(cudaGetLastError(), "run_compact_kernel");
+    // pairs per block: the run index at each block's first entry
+    std::vector<int64_t> pair_off(static_cast<size_t>(nb) + 1);
+    {
+        const std::vector<int64_t> h_pos = to_host(pos, static_cast<size_t>(ne), s);
+        for (int64_t b = 0; b < nb; ++b) pair_off[b] = boff64[b] < ne ? h_pos[boff64[b]] : n_runs;
+        pair_off[nb] = n_runs;
+        // an empty block has no runs: its offset is the next block's
+        for (int64_t b = nb - 1; b >= 0; --b)
+            if (boff64[b] == boff64[b + 1]) pair_off[b] = pair_off[b + 1];
+    }
+    flag.reset();
+    pos.reset();
+    DevArray<float> delta(ne);
+    DevArray<uint8_t> has_delta(ne);
+    DevArray<uint64_t> pkey(std::max<int64_t>(n_runs, 1)), pkey2(std::max<int64_t>(n_runs, 1));
+    DevArray<int32_t> pblock(std::max<int64_t>(n_runs, 1));
+    runs_kernel<ESZ><<<sms * 8, 256, 0, s>>>(skey.data(), sidx.data(), eval.data(), run_start.data(),
+                                             n_runs, ne, entry_block.data(), delta.data(),
+                                             has_delta.data(), pkey.data(), pblock.data());
+    cuda_check(cudaGetLastError(), "runs_kernel");
+    DevArray<float> mass(nb);
+    mass_kernel<<<sms * 4, 128, 0, s>>>(delta.data(), has_delta.data(), d_boff.data(), nb,
+                                        mass.data());
+    cuda_check(cudaGetLastError(), "mass_kernel");
+    // alpha cut over each block's maxima, value descending
+    DevArray<int32_t> d_pair_off32;
+    to_dev(d_pair_off32, to_i32_offsets(pair_off), s);
+    segmented_sort_keys(pkey.data(), pkey2.data(), n_runs, nb, d_pair_off32.data(), s);
+    DevArray<int64_t> d_pair_off;
+    to_dev(d_pair_off, pair_off, s);
+    DevArray<int32_t> keep(nb);
+    cut_kernel<<<sms * 4, 128, 0, s>>>(pkey2.data(), d_pair_off.data(), nb, mass.data(), alpha,
+                                       keep.data());
+    cuda_check(cudaGetLastError(), "cut_kernel");
+    const std::vector<int32_t> h_keep = to_host(keep, static_cast<size_t>(nb), s);
+    std::vector<int64_t> kept_off(static_cast<size_t>(nb) + 1, 0);
+    for (int64_t b = 0; b < nb; ++b) kept_off[b + 1] = kept_off[b] + h_keep[b];
+    const int64_t n_kept = kept_off[nb];
+    std::vector<uint16_t> block_local(static_cast<size_t>(nb));
+    std::vector<int64_t> list_koff(static_cast<size_t>(t1 - t0) + 1, 0);
+    for (int32_t t = t0; t < t1; ++t) {
+        for (int64_t b = L.lbp[t]; b < L.lbp[t + 1]; ++b)
+            block_local[b - b0] = static_cast<uint16_t>(b - L.lbp[t]);
+        list_koff[t - t0 + 1] = kept_off[L.lbp[t + 1] - b0];
+    }
+    DevArray<int64_t> d_kept_off;
+    to_dev(d_kept_off, kept_off, s);
+    DevArray<uint16_t> d_block_local;
+    to_dev(d_block_local, block_local, s);
+    DevArray<uint32_t> tkey(std::max<int64_t>(n_kept, 1)), tkey2(std::max<int64_t>(n_kept, 1));
+    DevArray<float> tval(std::max<int64_t>(n_kept, 1)), tval2(std::max<int64_t>(n_kept, 1));
+    kept_pairs_kernel<<<sms * 8, 128, 0, s>>>(pkey2.data(), d_pair_off.data(), keep.data(),
+                                              d_kept_off.data(), d_block_local.data(), nb,
+                                              tkey.data(), tval.data());
+    cuda_check(cudaGetLastError(), "kept_pairs_kernel");
+    // term-major per list (build_transpose, inverted_list_clusters.cpp:230-293)
+    DevArray<int32_t> d_list_koff;
+    to_dev(d_list_koff, to_i32_offsets(list_koff), s);
+    segmented_sort_pairs(tkey.data(), tkey2.data(), tval.data(), tval2.data(), n_kept, t1 - t0,
+                         d_list_koff.data(), s, /*stable=*/false);
+    const std::vector<uint32_t> hk = to_host(tkey2, static_cast<size_t>(n_kept), s);
+    const std::vector<float> hv = to_host(tval2, static_cast<size_t>(n_kept), s);
+    for (int32_t t = t0; t < t1; ++t) {
+        const int64_t k0 = list_koff[t - t0], k1 = list_koff[t - t0 + 1];
+        for (int64_t i = k0; i < k1; ++i) {
+            const uint16_t term = static_cast<uint16_t>(hk[i] >> 16);
+            if (i == k0 || term != static_cast<uint16_t>(hk[i - 1] >> 16)) {
+                L.sterm.push_back(term);
+                L.srun.push_back(L.srun.back());
+            }
+            L.srun.back() += 1;
+            L.sblk.push_back(static_cast<uint16_t>(hk[i] & 0xffffu));
+            if constexpr (ESZ == 4) {
+                const uint8_t* b = reinterpret_cast<const uint8_t*>(&hv[i]);
+                L.sval.insert(L.sval.end(), b, b + 4);
+            } else if constexpr (ESZ == 2) {
+                const uint16_t c = static_cast<uint16_t>(hv[i]);
+                const uint8_t* b = reinterpret_cast<const uint8_t*>(&c);
+                L.sval.insert(L.sval.end(), b, b + 2);
+            } else {
+                L.sval.push_back(static_cast<uint8_t>(hv[i]));
+            }
+        }
+        L.ltp.push_back(static_cast<int64_t>(L.sterm.size()));
+    }
+}
+
+template <int ESZ>
+void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
+    const nsp::HostCsr& h = st.vectors.host;
+    cudaStream_t s = nsp::Workspace::get().stream();
+    const int64_t n_docs = h.n();
+    const int lambda = calc_lambda(p.lambda, static_cast<size_t>(n_docs));
+    const int beta = calc_beta(p.beta, lambda);
+    const int64_t cap = lambda <= 0 ? 0 : lambda;  // 0: keep whole lists (inverted_lists.cpp:114)
+    const uint32_t base_seed =
+        p.seed == -1 ? std::random_device{}() : static_cast<uint32_t>(p.seed);
+    st.vectors.ensure_device();
+    const nsp::FwdView f = st.vectors.dev.view();
+    const int32_t n_lists = dim;
+    const int sms = nsp::device_sm_count();
+
+    // ---- 1. postings
+    DevArray<unsigned long long> cnt(static_cast<size_t>(n_lists) + 1);
+    cuda_check(cudaMemsetAsync(cnt.data(), 0, cnt.size() * 8, s), "memset");
+    post_count_kernel<<<sms * 8, 256, 0, s>>>(f, cnt.data());
+    cuda_check(cudaGetLastError(), "post_count_kernel");
+    DevArray<int64_t> post_ptr(static_cast<size_t>(n_lists) + 1);
+    nsp::exclusive_scan_i64(reinterpret_cast<const int64_t*>(cnt.data()), post_ptr.data(),
+                            n_lists + 1, s);
+    const std::vector<int64_t> h_post = to_host(post_ptr, n_lists + 1, s);
+    const int64_t nnz = h_post.back();
+    DevArray<uint64_t> keys(static_cast<size_t>(std::max<int64_t>(nnz, 1)));
+    DevArray<uint64_t> keys2(static_cast<size_t>(std::max<int64_t>(nnz, 1)));
+    cuda_check(cudaMemsetAsync(cnt.data(), 0, cnt.size() * 8, s), "memset");
+    post_scatter_kernel<ESZ><<<sms * 8, 256, 0, s>>>(f, post_ptr.data(), cnt.data(), cap, keys.data());
+    cuda_check(cudaGetLastError(), "post_scatter_kernel");
+    {
+        DevArray<int32_t> off32;
+        to_dev(off32, to_i32_offsets(h_post), s);
+        segmented_sort_keys(keys.data(), keys2.data(), nnz, n_lists, off32.data(), s);
+    }
+    keys.reset();
+    std::vector<int32_t> kept_len(n_lists);
+    std::vector<int64_t> kept_ptr(n_lists + 1, 0);
+    for (int32_t t = 0; t < n_lists; ++t) {
+        const int64_t len = h_post[t + 1] - h_post[t];
+        kept_len[t] = static_cast<int32_t>(cap > 0 && len > cap ? cap : len);
+        kept_ptr[t + 1] = kept_ptr[t] + kept_len[t];
+    }
+    const int64_t total_kept = kept_ptr.back();
+    DevArray<int64_t> d_kept_ptr;
+    to_dev(d_kept_ptr, kept_ptr, s);
+    DevArray<int32_t> kept(static_cast<size_t>(std::max<int64_t>(total_kept, 1)));
+    kept_copy_kernel<<<sms * 8, 256, 0, s>>>(keys2.data(), post_ptr.data(), d_kept_ptr.data(),
+                                             n_lists, kept.data());
+    cuda_check(cudaGetLastError(), "kept_copy_kernel");
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    keys2.reset();
+
+    // ---- 2. centroid positions (host; depends on list lengths only)
+    std::vector<int64_t> cptr(n_lists + 1, 0);
+    for (int32_t t = 0; t < n_lists; ++t)
+        cptr[t + 1] = cptr[t] + (kept_len[t] > 0 ? static_cast<int64_t>(clusters_for(kept_len[t], beta)) : 0);
+    int32_t max_nc = 0;
+    int64_t max_kept = 0;
+    for (int32_t t = 0; t < n_lists; ++t) {
+        max_nc = std::max<int32_t>(max_nc, static_cast<int32_t>(cptr[t + 1] - cptr[t]));
+        max_kept = std::max<int64_t>(max_kept, kept_len[t]);
+    }
+    if (max_nc > 65536)
+        throw std::invalid_argument("more than 65536 blocks in one posting list");
+    std::vector<int32_t> cpos(static_cast<size_t>(std::max<int64_t>(cptr.back(), 1)));
+    {
+        const int nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        for (int w = 0; w < nth; ++w) {
+            pool.emplace_back([&, w] {
+                std::vector<int32_t> perm;
+                for (int32_t t = w; t < n_lists; t += nth) {
+                    if (kept_len[t] == 0) continue;
+                    draw_positions(static_cast<size_t>(kept_len[t]),
+                                   static_cast<size_t>(cptr[t + 1] - cptr[t]),
+                                   base_seed + static_cast<uint32_t>(t), perm, cpos.data() + cptr[t]);
+                }
+            });
+        }
+        for (auto& th : pool) th.join();
+    }
+    DevArray<int64_t> d_cptr;
+    DevArray<int32_t> d_cpos;
+    to_dev(d_cptr, cptr, s);
+    to_dev(d_cpos, cpos, s);
+
+    // ---- 3. assignment
+    DevArray<uint32_t> akey(static_cast<size_t>(std::max<int64_t>(total_kept, 1)));
+    if (total_kept > 0) {
+        // centroid entries per list bound: max_nc rows of the longest rows
+        int64_t max_row = 0;
+        for (int64_t d = 0; d < n_docs; ++d)
+            max_row = std::max<int64_t>(max_row, h.indptr[d + 1] - h.indptr[d]);
+        const int64_t max_ce = std::max<int64_t>(1, static_cast<int64_t>(max_nc) * max_row);
+        const int ctas = sms * 2;
+        const int wpb = 8;
+        DevArray<int32_t> tcnt(static_cast<size_t>(ctas) * dim), tstart(static_cast<size_t>(ctas) * dim),
+            tcur(static_cast<size_t>(ctas) * dim), touched(static_cast<size_t>(ctas) * max_ce);
+        DevArray<uint16_t> ccl(static_cast<size_t>(ctas) * max_ce);
+        DevArray<uint8_t> cw(static_cast<size_t>(ctas) * max_ce * ESZ);
+        DevArray<uint8_t> isc(static_cast<size_t>(ctas) * std::max<int64_t>(max_kept, 1));
+        DevArray<uint8_t> sims(static_cast<size_t>(ctas) * wpb * std::max(max_nc, 1) * 8);
+        DevArray<int32_t> work(1);
+        cuda_check(cudaMemsetAsync(tcnt.data(), 0, tcnt.size() * 4, s), "memset");
+        cuda_check(cudaMemsetAsync(work.data(), 0, 4, s), "memset");
+        AssignArgs a{};
+        a.f = f;
+        a.n_lists = n_lists;
+        a.kept_ptr = d_kept_ptr.data();
+        a.kept = kept.data();
+        a.cptr = d_cptr.data();
+        a.cpos = d_cpos.data();
+        a.out_key = akey.data();
+        a.work = work.data();
+        a.tcnt = tcnt.data();
+        a.tstart = tstart.data();
+        a.tcur = tcur.data();
+        a.touched = touched.data();
+        a.ccl = ccl.data();
+        a.cw = cw.data();
+        a.is_centroid = isc.data();
+        a.sims = sims.data();
+        a.max_centroid_entries = max_ce;
+        a.max_kept = std::max<int64_t>(max_kept, 1);
+        a.max_nc = std::max(max_nc, 1);
+        assign_kernel<ESZ><<<ctas, wpb * 32, 0, s>>>(a);
+        cuda_check(cudaGetLastError(), "assign_kernel");
+        cuda_check(cudaStreamSynchronize(s), "assign sync");
+    }
+
+    // ---- 4. blocks: centroid first, members in list order
+    DevArray<int32_t> bdocs(static_cast<size_t>(std::max<int64_t>(total_kept, 1)));
+    DevArray<uint32_t> akey2(static_cast<size_t>(std::max<int64_t>(total_kept, 1)));
+    {
+        DevArray<int32_t> off32;
+        to_dev(off32, to_i32_offsets(kept_ptr), s);
+        segmented_sort_pairs(akey.data(), akey2.data(), kept.data(), bdocs.data(), total_kept,
+                             n_lists, off32.data(), s, /*stable=*/true);
+    }
+    const std::vector<uint32_t> h_akey = to_host(akey2, static_cast<size_t>(total_kept), s);
+    akey.reset();
+    akey2.reset();
+    kept.reset();
+    nsp::SeismicHost L;
+    L.esz = ESZ;
+    L.lbp.assign(1, 0);
+    L.bdp.assign(1, 0);
+    L.docs = to_host(bdocs, static_cast<size_t>(total_kept), s);
+    for (int32_t t = 0; t < n_lists; ++t) {
+        const int64_t nc = cptr[t + 1] - cptr[t];
+        L.lbp.push_back(L.lbp.back() + nc);
+        int64_t i = kept_ptr[t];
+        for (int64_t c = 0; c < nc; ++c) {
+            while (i < kept_ptr[t + 1] && static_cast<int64_t>(h_akey[i] >> 1) == c) ++i;
+            L.bdp.push_back(i);
+        }
+    }
+    const int64_t n_blocks = L.lbp.back();
+
+    // ---- 5. summaries, in batches of lists bounded by entry count
+    std::vector<int64_t> doc_len(static_cast<size_t>(total_kept));
+    for (int64_t j = 0; j < total_kept; ++j) {
+        const int32_t d = L.docs[j];
+        doc_len[j] = h.indptr[d + 1] - h.indptr[d];
+    }
+    std::vector<int64_t> doc_eoff(static_cast<size_t>(total_kept) + 1, 0);
+    for (int64_t j = 0; j < total_kept; ++j) doc_eoff[j + 1] = doc_eoff[j] + doc_len[j];
+    std::vector<int64_t> blk_e(static_cast<size_t>(n_blocks) + 1, 0);
+    for (int64_t b = 0; b <= n_blocks; ++b) blk_e[b] = doc_eoff[L.bdp[b]];
+    DevArray<int64_t> d_bdp;
+    to_dev(d_bdp, L.bdp, s);
+    DevArray<int32_t> d_docs;
+    to_dev(d_docs, L.docs, s);
+    const int64_t budget = int64_t{1} << 27;  // entries per batch
+    L.ltp.assign(1, 0);
+    L.srun.assign(1, 0);
+    L.sterm.clear();
+    L.sblk.clear();
+    L.sval.clear();
+    int32_t t0 = 0;
+    while (t0 < n_lists) {
+        int32_t t1 = t0 + 1;
+        while (t1 < n_lists && blk_e[L.lbp[t1 + 1]] - blk_e[L.lbp[t0]] <= budget) ++t1;
+        const int64_t b0 = L.lbp[t0], b1 = L.lbp[t1];
+        const int64_t nb = b1 - b0;
+        const int64_t e0 = blk_e[b0], ne = blk_e[b1] - e0;
+        if (nb == 0 || ne == 0) {
+            for (int32_t t = t0; t < t1; ++t) L.ltp.push_back(L.ltp.back());
+            t0 = t1;
+            continue;
+        }
+        summarize_batch<ESZ>(f, d_docs, d_bdp, L, t0, t1, doc_eoff, blk_e, p.alpha, s);
+        t0 = t1;
+    }
+
+    // ---- 6. publish
+    std::lock_guard<std::mutex> g(st.mu);
+    st.lists = std::move(L);
+    st.list_esz.assign(static_cast<size_t>(n_lists), static_cast<uint8_t>(ESZ));
+    st.host_valid = true;
+    st.dev_valid = false;
+}
+
+}  // namespace
+
+void seismic_build(SeismicState& st, int dim, const SeismicClusterParameters& params) {
+    for (uint16_t t : st.vectors.host.indices)
+        if (t >= dim) throw std::invalid_argument("term_id out of range");
+    const int esz = st.vectors.host.esz;
+    if (st.vectors.host.n() == 0) {
+        // no documents: one empty list per term
+        nsp::SeismicHost L;
+        L.esz = esz;
+        L.lbp.assign(static_cast<size_t>(dim) + 1, 0);
+        L.ltp.assign(static_cast<size_t>(dim) + 1, 0);
+        std::lock_guard<std::mutex> g(st.mu);
+        st.lists = std::move(L);
+        st.list_esz.assign(static_cast<size_t>(dim), static_cast<uint8_t>(esz));
+        st.host_valid = true;
+        st.dev_valid = false;
+        return;
+    }
+    if (esz == 4) build_typed<4>(st, dim, params);
+    else if (esz == 2) build_typed<2>(st, dim, params);
+    else build_typed<1>(st, dim, params);
 }
 
 }  // namespace detail

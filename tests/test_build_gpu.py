@@ -1,0 +1,165 @@
+"""The SEISMIC build on the device against the reference's build.
+
+fp32: with a fixed seed the device-built index file is byte-identical to the
+one the reference writes (posting truncation, centroid draw, assignment,
+summaries and transposes all agree) wherever no two values tie.
+
+uint8 (SEISMIC-SQ): codes tie constantly, and the reference breaks ties in its
+posting truncation and summary cut with an unstable sort, so whole files are
+not comparable. Instead each list is checked through the reference's own
+functions: given the engine's kept list and centroids, the reference's
+assigner (cluster/kmeans_utils.cpp) produces the engine's blocks exactly, and
+its summarizer (cluster/inverted_list_clusters.cpp) produces summaries with
+the engine's entry counts and values.
+"""
+
+import hashlib
+
+import numpy as np
+import pytest
+
+import nsparse
+import oracle as O
+from helpers import CUT, HF, K, SEISMIC, golden, golden_corpus, recall, ref_file, sq_spec
+from nsparse_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def device_build(docs, spec, path=None):
+    idx = nsparse.index_factory(docs.dim, spec)
+    idx.add(docs.n, docs.indptr, docs.indices, docs.values)
+    idx.build()
+    if path is not None:
+        nsparse.write_index(idx, str(path))
+    return idx
+
+
+def sha(path):
+    return hashlib.sha256(open(path, "rb").read()).hexdigest()
+
+
+def test_fp32_build_is_byte_identical_to_reference_golden(tmp_path):
+    g = golden()
+    docs, qs = golden_corpus()
+    idx = device_build(docs, SEISMIC, tmp_path / "d.idx")
+    assert sha(tmp_path / "d.idx") == str(g["seismic_file_sha"])
+    D, L = idx.search(qs.n, qs.indptr, qs.indices, qs.values, K,
+                      nsparse.SeismicSearchParameters(CUT, HF))
+    np.testing.assert_array_equal(L, g["seismic_L"])
+    np.testing.assert_array_equal(D, g["seismic_D"])
+
+
+@pytest.mark.parametrize("spec", [
+    "seismic,lambda=400|beta=40|alpha=0.4|seed=7",
+    "seismic,lambda=-1|beta=-1|alpha=0.5|seed=3",
+    "seismic,lambda=50|beta=0|alpha=0.2|seed=11",
+    "seismic,lambda=0|beta=8|alpha=0.9|seed=5",
+])
+def test_fp32_build_matches_reference_file(tmp_path, spec):
+    docs = synth.docs_config0(20000, seed=3)
+    ref_file(docs, spec, tmp_path / "r.idx")
+    device_build(docs, spec, tmp_path / "d.idx")
+    a = open(tmp_path / "r.idx", "rb").read()
+    b = open(tmp_path / "d.idx", "rb").read()
+    assert len(a) == len(b)
+    assert a == b
+
+
+def test_seeded_build_is_reproducible_and_seed_matters(tmp_path):
+    docs, qs = golden_corpus()
+    device_build(docs, SEISMIC, tmp_path / "a.idx")
+    device_build(docs, SEISMIC, tmp_path / "b.idx")
+    assert sha(tmp_path / "a.idx") == sha(tmp_path / "b.idx")
+    device_build(docs, SEISMIC.replace("seed=7", "seed=8"), tmp_path / "c.idx")
+    assert sha(tmp_path / "a.idx") != sha(tmp_path / "c.idx")
+
+
+def _posting_codes(docs, codes, t):
+    rows = np.repeat(np.arange(docs.n), np.diff(docs.indptr))
+    m = docs.indices == t
+    return rows[m].astype(np.int32), codes[m]
+
+
+def test_sq_build_assignment_and_summaries_match_reference(tmp_path):
+    docs, _ = golden_corpus()
+    vmin, vmax = float(docs.values.min()), float(docs.values.max())
+    lam, beta, alpha = 200, 20, 0.4
+    device_build(docs, sq_spec(vmin, vmax, lam, beta), tmp_path / "q.idx")
+    f = O.read_index_file(str(tmp_path / "q.idx"))
+    codes = O.sq_encode_u8(vmin, vmax, docs.values)
+    L = O.ref_lib("generic")
+    P = lambda a: a.ctypes.data  # noqa: E731
+    lists = f["lists"]
+    checked = 0
+    rng = np.random.default_rng(0)
+    cand = [t for t, c in enumerate(lists) if c["n_clusters"] >= 2]
+    for t in rng.choice(cand, size=min(120, len(cand)), replace=False):
+        c = lists[t]
+        ids, vals = _posting_codes(docs, codes, t)
+        if len(ids) > lam:
+            order = np.lexsort((ids, -vals.astype(np.int64)))[:lam]
+            kept = ids[order]
+        else:
+            kept = ids
+        off = c["offsets"]
+        blocks = [c["docs"][off[b]:off[b + 1]] for b in range(len(off) - 1)]
+        assert sorted(np.concatenate(blocks).tolist()) == sorted(kept.tolist())
+        cents = np.array([b[0] for b in blocks], np.int32)
+        out_docs = np.empty(len(kept), np.int32)
+        out_off = np.empty(len(cents) + 1, np.int32)
+        kept = np.ascontiguousarray(kept, np.int32)
+        assert L.ref_map_docs_to_clusters(docs.dim, 1, docs.n, P(docs.indptr), P(docs.indices),
+                                          P(codes), P(kept), len(kept), P(cents), len(cents),
+                                          P(out_docs), P(out_off)) == 0
+        ref_blocks = [out_docs[out_off[b]:out_off[b + 1]] for b in range(len(cents))]
+        for mine, theirs in zip(blocks, ref_blocks):
+            np.testing.assert_array_equal(mine, theirs)
+        # summaries of these clusters
+        cap = 1 << 22
+        buf = np.empty(cap, np.uint8)
+        n = L.ref_summarize(docs.dim, 1, docs.n, P(docs.indptr), P(docs.indices), P(codes),
+                            P(c["docs"]), P(off), len(off) - 1, alpha, P(buf), cap)
+        assert n > 0
+        r = O._read_clusters(O._Rd(bytes(buf[:n])))
+        mine_cnt = np.bincount(c["csc_cluster"], minlength=len(off) - 1)
+        ref_cnt = np.bincount(r["csc_cluster"], minlength=len(off) - 1)
+        np.testing.assert_array_equal(mine_cnt, ref_cnt)
+        for b in range(len(off) - 1):
+            mv = np.sort(c["csc_value"][c["csc_cluster"] == b])
+            rv = np.sort(r["csc_value"][r["csc_cluster"] == b])
+            np.testing.assert_array_equal(mv, rv)
+        checked += 1
+    assert checked > 50
+
+
+def test_sq_build_search_recall_matches_reference(tmp_path):
+    docs = synth.docs_config0(20000, seed=4)
+    qs = synth.queries_config0(200, seed=4)
+    vmin, vmax = float(docs.values.min()), float(docs.values.max())
+    spec = sq_spec(vmin, vmax, 400, 40)
+    idx = device_build(docs, spec)
+    r = ref_file(docs, spec, tmp_path / "r.idx")
+    D, L = idx.search(qs.n, qs.indptr, qs.indices, qs.values, K,
+                      nsparse.SeismicSearchParameters(10, 0.8))
+    _, Lr = r.search(qs, K, param_kind=2, cut=10, heap_factor=0.8)
+    _, Lt = O.exact_search(docs, qs, K, 1)
+    assert recall(L, Lt) >= recall(Lr, Lt) - 0.01
+
+
+def test_build_rejects_out_of_range_terms():
+    docs, _ = golden_corpus()
+    idx = nsparse.index_factory(1000, SEISMIC)
+    idx.add(docs.n, docs.indptr, docs.indices, docs.values)
+    with pytest.raises(ValueError, match="term_id out of range"):
+        idx.build()
+
+
+def test_build_of_tiny_and_empty_inputs(tmp_path):
+    docs, qs = golden_corpus()
+    small = docs.rows(0, 3)
+    idx = device_build(small, SEISMIC, tmp_path / "s.idx")
+    ref_file(small, SEISMIC, tmp_path / "r.idx")
+    assert sha(tmp_path / "s.idx") == sha(tmp_path / "r.idx")
+    D, L = idx.search(qs.n, qs.indptr, qs.indices, qs.values, 10)
+    assert (L[:, 3:] == -1).all()
