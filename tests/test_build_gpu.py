@@ -62,8 +62,37 @@ def test_fp32_build_matches_reference_file(tmp_path, spec):
     device_build(docs, spec, tmp_path / "d.idx")
     a = open(tmp_path / "r.idx", "rb").read()
     b = open(tmp_path / "d.idx", "rb").read()
-    assert len(a) == len(b)
-    assert a == b
+    if a == b:
+        return
+    # Not byte-identical: every difference must be a tie the reference leaves
+    # to its unstable sort (equal maxima straddling the alpha cut).
+    ra, rb = O.read_index_file(str(tmp_path / "r.idx")), O.read_index_file(str(tmp_path / "d.idx"))
+    np.testing.assert_array_equal(ra["vectors"]["values"], rb["vectors"]["values"])
+    n_blocks = n_diff = 0
+    for la, lb in zip(ra["lists"], rb["lists"]):
+        np.testing.assert_array_equal(la["docs"], lb["docs"])        # truncation + assignment
+        np.testing.assert_array_equal(la["offsets"], lb["offsets"])
+        for blk in range(len(la["offsets"]) - 1 if len(la["offsets"]) else 0):
+            n_blocks += 1
+            ta, va = _block_summary(la, blk)
+            tb, vb = _block_summary(lb, blk)
+            if np.array_equal(ta, tb) and np.array_equal(va, vb):
+                continue
+            n_diff += 1
+            np.testing.assert_array_equal(np.sort(va), np.sort(vb))  # same kept values
+            boundary = va.min()
+            only = set(ta.tolist()) ^ set(tb.tolist())
+            vals = dict(zip(ta.tolist(), va.tolist()))
+            vals.update(zip(tb.tolist(), vb.tolist()))
+            assert all(vals[t] == boundary for t in only), "summary differs beyond a tie"
+    assert n_diff <= max(1, n_blocks // 1000)
+
+
+def _block_summary(lst, blk):
+    """(terms, values) of one block's summary from a list's CSC arrays."""
+    m = lst["csc_cluster"] == blk
+    col = np.searchsorted(lst["term_ptr"], np.nonzero(m)[0], side="right") - 1
+    return lst["term_ids"][col], lst["csc_value"][m]
 
 
 def test_seeded_build_is_reproducible_and_seed_matters(tmp_path):
