@@ -148,6 +148,35 @@ nsp_status_t nsp_index_search_device(nsp_index_t* index, int32_t n, const int32_
                                      int32_t* d_labels, const nsp_search_params_t* params,
                                      void* cuda_stream);
 
+/* SEISMIC search that allocates nothing. No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory per call: an engine
+ * embedded in a host whose allocator accounts for every device byte against
+ * a fixed budget, or a latency-critical loop that cannot afford
+ * cudaMalloc/cudaFree, which can synchronize the device. Same arguments and
+ * results as nsp_index_search_device, plus `nnz` (= d_indptr[n], the number
+ * of query entries). The kernel's scratch (work counter, encoded query codes,
+ * per-warp block-score rows) lives in a fixed device array of
+ * NSP_NOALLOC_SCRATCH_BYTES that every GPU loading the library reserves until
+ * exit; no cudaMalloc, cudaFree or allocating library routine is called.
+ *   - The first call on a device looks up that array's device address (set-up
+ *     once per device); make that first call before any stream capture.
+ *   - The index must already be resident on the GPU (one ordinary search or a
+ *     build followed by a search does that); otherwise the call is rejected.
+ *   - Rejected with NSP_ERR_INVALID_ARGUMENT: an id selector, plain mode, or a
+ *     batch whose codes (2*nnz bytes) or block-score rows (4 bytes per block of
+ *     the largest posting list, per warp) do not fit the array.
+ *   - All calls share the array and it keeps the last call's contents: calls
+ *     that overlap on the GPU (other streams, other host threads) race; order
+ *     them on one stream. */
+#define NSP_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+nsp_status_t nsp_index_search_device_noalloc(nsp_index_t* index, int32_t n,
+                                             const int32_t* d_indptr, const uint16_t* d_indices,
+                                             const float* d_values, int32_t nnz,
+                                             int32_t max_row_nnz, int k, float* d_distances,
+                                             int32_t* d_labels, const nsp_search_params_t* params,
+                                             void* cuda_stream);
+
 /* Number of CUDA devices visible and the name of the current one. */
 nsp_status_t nsp_device_info(int32_t* n_devices, char* name, size_t name_len);
 

@@ -67,6 +67,11 @@ void check_out(T** out) {
 
 }  // namespace
 
+namespace nsp {
+// Lets entry points defined in other files report through nsp_last_error.
+void set_last_error(const char* msg) { g_error = msg; }
+}  // namespace nsp
+
 extern "C" {
 
 const char* nsp_last_error(void) { return g_error.c_str(); }
