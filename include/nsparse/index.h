@@ -20,6 +20,11 @@ namespace nsparse {
 struct EngineOptions {
     bool plain = false;
     int warps_per_block = 0;
+    // SEISMIC kernel variant: -1 lets the engine choose, 0 loads doc rows
+    // straight from HBM, 1 stages them in shared memory by bulk copy
+    // (stage_bytes per buffer, 0 = default). Results are identical.
+    int variant = -1;
+    int stage_bytes = 0;
 };
 
 struct SearchParameters {

@@ -237,6 +237,18 @@ nsp_status_t nsp_search_params_set_engine(nsp_search_params_t* params, int plain
     });
 }
 
+nsp_status_t nsp_search_params_set_kernel(nsp_search_params_t* params, int variant,
+                                          int stage_bytes) {
+    return guarded([&] {
+        if (params == nullptr) throw std::invalid_argument("unexpected nullptr");
+        if (variant < -1 || variant > 1) throw std::invalid_argument("variant must be -1, 0 or 1");
+        if (stage_bytes < 0 || stage_bytes > (96 << 10))
+            throw std::invalid_argument("stage_bytes must be in [0, 98304]");
+        as_params(params)->engine.variant = variant;
+        as_params(params)->engine.stage_bytes = stage_bytes;
+    });
+}
+
 nsp_status_t nsp_search_params_free(nsp_search_params_t* params) {
     return guarded([&] { delete as_params(params); });
 }

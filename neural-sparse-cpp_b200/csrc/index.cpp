@@ -75,6 +75,8 @@ nsp::SeismicSearchArgs seismic_args(const SearchParameters* p, int k) {
     if (p != nullptr) {
         a.plain = p->engine.plain;
         a.warps_per_block = p->engine.warps_per_block;
+        a.variant = p->engine.variant;
+        a.stage_bytes = p->engine.stage_bytes;
     }
     return a;
 }

@@ -91,6 +91,13 @@ struct SeismicLaunch {
     float* bscore;              // scratch: per warp slot, max_blocks floats
     unsigned long long* stats;  // kStatCount counters, or nullptr
     int32_t first_query;        // static mode: queries first_query.. strided
+    // Variant 1 (staged): doc rows arrive in shared memory by bulk copy,
+    // double-buffered, stage_bytes per buffer; block scores of lists with at
+    // most bcap blocks stay in shared memory. Variant 0 loads rows directly.
+    int32_t variant;
+    int32_t stage_bytes;
+    int32_t bcap;
+    int32_t* err;               // set to 1 when a bounded wait gives up
 };
 
 struct ExactLaunch {
@@ -113,10 +120,12 @@ struct ExactLaunch {
 
 // Launchers (return cudaError_t of the launch). `sm_count` sizes persistent
 // grids; `plan_*` report the dynamic shared memory a launch needs.
-size_t seismic_smem_per_warp(int val_kind, int dim_words, int qcap, int k);
+size_t seismic_smem_per_warp(int val_kind, int dim_words, int qcap, int k, int bcap = 0,
+                             int stage_bytes = 0);
 cudaError_t launch_seismic(int val_kind, const SeismicLaunch& a, int warps_per_block,
                            int blocks, cudaStream_t s);
-int seismic_max_blocks_per_sm(int val_kind, int warps_per_block, size_t smem);
+int seismic_max_blocks_per_sm(int val_kind, int variant, int warps_per_block, size_t smem);
+int seismic_max_blocks_per_sm(int val_kind, int warps_per_block, size_t smem);  // variant 0
 
 size_t exact_smem(int dim_words, int qcap_smem);  // qcap_smem 0: values in global
 cudaError_t launch_exact(const ExactLaunch& a, int tiles, cudaStream_t s);

@@ -31,6 +31,7 @@
 #include <cstdint>
 
 #include "nsp_device.h"
+#include "tma.h"
 
 namespace nsp {
 namespace {
@@ -69,9 +70,18 @@ struct WarpSlice {
     uint32_t* coff;    // [32]
     uint32_t* clen;    // [32]
     float* csc;        // [32]
+    // staged variant only (nullptr otherwise)
+    float* bscore_s;        // [bcap] block scores of the current list
+    unsigned char* sbuf;    // [2][stage_bytes] bulk-copied doc rows
+    uint64_t* mbar;         // [2]
+    int32_t* sdoc;          // [2][32] docs of each staged chunk, list order
+    uint32_t* slen;         // [2][32] their row lengths
+    uint32_t* soff;         // [2][32] their byte offsets in the stage buffer
+    int32_t* smeta;         // [2][2] doc count, direct flag per buffer
 };
 
-__host__ __device__ inline size_t slice_bytes(int vsize, int words, int qcap, int k) {
+__host__ __device__ inline size_t slice_bytes(int vsize, int words, int qcap, int k, int bcap = 0,
+                                              int stage_bytes = 0) {
     size_t b = 0;
     b += ((size_t)words * 4 + 15) & ~size_t(15);
     b += ((size_t)words * 2 + 15) & ~size_t(15);
@@ -82,13 +92,35 @@ __host__ __device__ inline size_t slice_bytes(int vsize, int words, int qcap, in
     b += ((size_t)k * 4 + 15) & ~size_t(15);
     b += 4 * 64 * 4;
     b += 32 * 4 * 4;
+    if (stage_bytes > 0) {
+        b += ((size_t)bcap * 4 + 15) & ~size_t(15);
+        b += 2 * (size_t)stage_bytes;
+        b += 16;                 // two mbarriers
+        b += 2 * 32 * 4 * 3;     // chunk descriptors
+        b += 16;                 // chunk meta
+    }
     return b;
 }
 
 template <typename V>
-__device__ WarpSlice<V> carve(unsigned char* base, int words, int qcap, int k) {
+__device__ WarpSlice<V> carve(unsigned char* base, int words, int qcap, int k, int bcap = 0,
+                              int stage_bytes = 0) {
     WarpSlice<V> w;
     size_t o = 0;
+    w.bscore_s = nullptr;
+    w.sbuf = nullptr;
+    w.mbar = nullptr;
+    if (stage_bytes > 0) {
+        // stage buffers first: bulk copies need 16-byte aligned destinations
+        w.sbuf = base + o;                                 o += 2 * (size_t)stage_bytes;
+        w.mbar = reinterpret_cast<uint64_t*>(base + o);    o += 16;
+        w.bscore_s = bcap > 0 ? reinterpret_cast<float*>(base + o) : nullptr;
+        o += align16((size_t)bcap * 4);
+        w.sdoc = reinterpret_cast<int32_t*>(base + o);     o += 2 * 32 * 4;
+        w.slen = reinterpret_cast<uint32_t*>(base + o);    o += 2 * 32 * 4;
+        w.soff = reinterpret_cast<uint32_t*>(base + o);    o += 2 * 32 * 4;
+        w.smeta = reinterpret_cast<int32_t*>(base + o);    o += 16;
+    }
     w.qbits = reinterpret_cast<uint32_t*>(base + o); o += align16((size_t)words * 4);
     w.qpre = reinterpret_cast<uint16_t*>(base + o);  o += align16((size_t)words * 2);
     w.qterm = reinterpret_cast<uint16_t*>(base + o); o += align16((size_t)qcap * 2);
@@ -369,9 +401,255 @@ __device__ void visit_block(const SeismicLaunch& a, const WarpSlice<V>& w, int64
     }
 }
 
+// ------------------------------------------------------ staged variant --
+// Rows of a block arrive in shared memory by bulk copy (cp.async.bulk), in
+// chunks that fill a stage buffer; two buffers alternate, so the next chunk is
+// in flight while the current one is scored. A row too long for a buffer is
+// scored straight from global memory, in its place in the block order.
+
+// Scores a row staged at `row` (ids, then values at row + 2 * padded len).
 template <typename V>
-__device__ void run_query(const SeismicLaunch& a, const WarpSlice<V>& w, float* bscore, int q,
-                          int lane) {
+__device__ float score_row_staged(const unsigned char* row, int len, int sub, unsigned submask,
+                                  const WarpSlice<V>& w, int sw) {
+    const int plen = (len + 15) & ~15;
+    const unsigned char* vrow = row + plen * 2;
+    if constexpr (sizeof(V) == 4) {
+        float acc = 0.0f;
+        float* stage = w.stage + sw * 64;
+        for (int e0 = 0; e0 < len; e0 += 64) {
+            const int e = e0 + sub * 8;
+            float p[8];
+            unsigned hm = 0u;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) p[u] = 0.0f;
+            if (e < len) {
+                uint32_t t[8];
+                unpack_terms(lds128(row + e * 2), t);
+                const uint4 a0 = lds128(vrow + e * 4);
+                const uint4 a1 = lds128(vrow + e * 4 + 16);
+                const float v[8] = {__uint_as_float(a0.x), __uint_as_float(a0.y),
+                                    __uint_as_float(a0.z), __uint_as_float(a0.w),
+                                    __uint_as_float(a1.x), __uint_as_float(a1.y),
+                                    __uint_as_float(a1.z), __uint_as_float(a1.w)};
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    if (e + u < len) {
+                        const int r = query_rank(w.qbits, w.qpre, t[u]);
+                        if (r >= 0) {
+                            p[u] = __fmul_rn(v[u], w.qval[r]);
+                            hm |= 1u << u;
+                        }
+                    }
+                }
+            }
+            const int hits = __popc(hm);
+            int incl = hits;
+#pragma unroll
+            for (int o = 1; o < 8; o <<= 1) {
+                const int y = __shfl_up_sync(submask, incl, o, 8);
+                if (sub >= o) incl += y;
+            }
+            const int total = __shfl_sync(submask, incl, 7, 8);
+            int c = incl - hits;
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (hm & (1u << u)) stage[c++] = p[u];
+            __syncwarp(submask);
+            if (sub == 0)
+                for (int h = 0; h < total; ++h) acc = __fadd_rn(acc, stage[h]);
+            __syncwarp(submask);
+        }
+        return acc;
+    } else {
+        long long acc = 0;
+        for (int e0 = 0; e0 < len; e0 += 64) {
+            const int e = e0 + sub * 8;
+            if (e < len) {
+                uint32_t t[8];
+                unpack_terms(lds128(row + e * 2), t);
+                uint32_t v[8];
+                if constexpr (sizeof(V) == 1) {
+                    const uint2 a0 = lds64(vrow + e);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) v[u] = (a0.x >> (8 * u)) & 0xffu;
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) v[4 + u] = (a0.y >> (8 * u)) & 0xffu;
+                } else {
+                    unpack_terms(lds128(vrow + e * 2), v);
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    if (e + u < len) {
+                        const int r = query_rank(w.qbits, w.qpre, t[u]);
+                        if (r >= 0)
+                            acc += static_cast<long long>(v[u]) * static_cast<long long>(w.qval[r]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) acc += __shfl_xor_sync(submask, acc, o, 8);
+        if (sizeof(V) == 1) return static_cast<float>(static_cast<int>(acc));
+        return static_cast<float>(acc);
+    }
+}
+
+// Takes block docs [pos, d1) into stage buffer `buf`: as many as fit, in order,
+// with the selector applied; issues their bulk copies. Returns the number of
+// doc-list entries consumed (a row larger than a buffer becomes a one-doc
+// "direct" chunk).
+template <typename V>
+__device__ int64_t issue_chunk(const SeismicLaunch& a, const WarpSlice<V>& w, int buf,
+                               int64_t pos, int64_t d1, int lane,
+                               unsigned long long& lane_bytes) {
+    constexpr int vsz = static_cast<int>(sizeof(V));
+    const uint32_t cap = static_cast<uint32_t>(a.stage_bytes);
+    const int64_t j = pos + lane;
+    const bool valid = j < d1;
+    const int32_t doc = valid ? __ldg(a.ix.docs + j) : -1;
+    bool member = valid;
+    if (member && a.sel_bits != nullptr) member = (__ldg(a.sel_bits + (doc >> 6)) >> (doc & 63)) & 1ull;
+    const uint2 ri = member ? __ldg(a.fwd.rowinfo + doc) : make_uint2(0u, 0u);
+    const uint32_t plen = (ri.y + 15u) & ~15u;
+    const uint32_t bytes = member ? plen * (2 + vsz) : 0u;
+    const bool big = bytes > cap;
+    uint32_t incl = bytes;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const unsigned brk = __ballot_sync(kFull, valid && (big || incl > cap));
+    const int64_t left = d1 - pos;
+    const int avail = left < 32 ? static_cast<int>(left) : 32;
+    const int c = brk ? __ffs(brk) - 1 : avail;
+    int32_t* sdoc = w.sdoc + buf * 32;
+    uint32_t* slen = w.slen + buf * 32;
+    uint32_t* soff = w.soff + buf * 32;
+    int32_t* meta = w.smeta + buf * 2;
+    uint64_t* bar = w.mbar + buf;
+    __syncwarp();
+    if (c == 0) {
+        // lane 0's row exceeds a buffer: score it from global memory
+        if (lane == 0) {
+            sdoc[0] = doc;
+            slen[0] = ri.y;
+            soff[0] = ri.x;
+            meta[0] = 1;
+            meta[1] = 1;
+            mbar_arrive_expect_tx(bar, 0u);
+            lane_bytes += 8ull + static_cast<unsigned long long>(ri.y) * (2 + vsz);
+        }
+        __syncwarp();
+        return 1;
+    }
+    const bool take = member && lane < c;
+    const unsigned tm = __ballot_sync(kFull, take);
+    const int p = __popc(tm & ((1u << lane) - 1u));
+    const uint32_t excl = incl - bytes;
+    if (take) {
+        sdoc[p] = doc;
+        slen[p] = ri.y;
+        soff[p] = excl;
+    }
+    const uint32_t total = __shfl_sync(kFull, incl, c - 1);
+    if (lane == 0) {
+        meta[0] = __popc(tm);
+        meta[1] = 0;
+    }
+    // the buffer's previous contents were read by this warp: order those
+    // reads before the copies that overwrite them
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (lane == 0) mbar_arrive_expect_tx(bar, total);
+    __syncwarp();
+    if (take && plen > 0) {  // an empty row needs no copy (and adds no bytes)
+        unsigned char* dst = w.sbuf + static_cast<size_t>(buf) * cap + excl;
+        const size_t e0 = static_cast<size_t>(ri.x) * kRowAlign;
+        bulk_copy_g2s(dst, a.fwd.idx + e0, plen * 2u, bar);
+        bulk_copy_g2s(dst + plen * 2u, static_cast<const unsigned char*>(a.fwd.val) + e0 * vsz,
+                      plen * static_cast<uint32_t>(vsz), bar);
+        lane_bytes += 8ull + static_cast<unsigned long long>(ri.y) * (2 + vsz);
+    }
+    __syncwarp();
+    return c;
+}
+
+// Waits for buffer `buf`, scores its docs and offers them to the heap in
+// order. False if the wait gave up (error recorded).
+template <typename V>
+__device__ bool process_chunk(const SeismicLaunch& a, const WarpSlice<V>& w, int buf,
+                              uint32_t& phase_bits, int& n, int lane,
+                              unsigned long long& docs_scored) {
+    const uint32_t phase = (phase_bits >> buf) & 1u;
+    if (!mbar_wait_bounded(w.mbar + buf, phase)) {
+        if (lane == 0 && a.err != nullptr) atomicExch(a.err, 1);
+        mbar_wait_bounded(w.mbar + buf, phase);  // let copies in flight land
+        return false;
+    }
+    phase_bits ^= 1u << buf;
+    const int32_t* meta = w.smeta + buf * 2;
+    const int cnt = meta[0];
+    const bool direct = meta[1] != 0;
+    const int32_t* sdoc = w.sdoc + buf * 32;
+    const uint32_t* slen = w.slen + buf * 32;
+    const uint32_t* soff = w.soff + buf * 32;
+    const int sw = lane >> 3;
+    const int sub = lane & 7;
+    const unsigned submask = 0xffu << (sw * 8);
+    if (direct) {
+        const float s = score_row<V>(a.fwd, soff[0], slen[0], sub, submask, w, sw);
+        if (lane == 0) w.csc[0] = s;
+    } else {
+        const unsigned char* base = w.sbuf + static_cast<size_t>(buf) * a.stage_bytes;
+        for (int g0 = 0; g0 < cnt; g0 += 4) {
+            const int gi = g0 + sw;
+            const bool act = gi < cnt;
+            const float s = score_row_staged<V>(base + (act ? soff[gi] : 0u),
+                                                act ? static_cast<int>(slen[gi]) : 0, sub,
+                                                submask, w, sw);
+            if (act && sub == 0) w.csc[gi] = s;
+        }
+    }
+    __syncwarp();
+    docs_scored += static_cast<unsigned long long>(cnt);
+    for (int i = 0; i < cnt; ++i) heap_offer(w.csc[i], sdoc[i], w.hs, w.hid, n, a.k, lane);
+    __syncwarp();
+    return true;
+}
+
+template <typename V>
+__device__ bool visit_block_staged(const SeismicLaunch& a, const WarpSlice<V>& w, int64_t B, int& n,
+                                   int lane, uint32_t& phase_bits, unsigned long long& docs_scored,
+                                   unsigned long long& bytes, unsigned long long& lane_bytes) {
+    const int64_t d0 = a.ix.bdp[B];
+    const int64_t d1 = a.ix.bdp[B + 1];
+    bytes += 16 + 4ull * static_cast<unsigned long long>(d1 - d0);
+    if (d1 <= d0) return true;
+    int buf = 0;
+    int64_t pos = d0 + issue_chunk<V>(a, w, buf, d0, d1, lane, lane_bytes);
+    for (;;) {
+        const bool more = pos < d1;
+        if (more) pos += issue_chunk<V>(a, w, buf ^ 1, pos, d1, lane, lane_bytes);
+        if (!process_chunk<V>(a, w, buf, phase_bits, n, lane, docs_scored)) {
+            // give the other buffer's copies a bounded chance to land, then stop
+            if (more) mbar_wait_bounded(w.mbar + (buf ^ 1), (phase_bits >> (buf ^ 1)) & 1u);
+            return false;
+        }
+        if (!more) return true;
+        buf ^= 1;
+    }
+}
+
+// Returns false if a bounded wait gave up (the query's results are then
+// padding and the warp stops).
+template <typename V, bool kStaged>
+__device__ bool run_query(const SeismicLaunch& a, const WarpSlice<V>& w, float* bscore_g, int q,
+                          int lane, uint32_t& phase_bits) {
+    // block scores of the current list: shared memory when they fit
+    float* bscore = (kStaged && w.bscore_s != nullptr && a.ix.max_blocks <= a.bcap) ? w.bscore_s
+                                                                                   : bscore_g;
+    bool ok = true;
     const int words = a.ix.words;
     const int32_t qs = a.q.indptr[q];
     const int qn = a.q.indptr[q + 1] - qs;
@@ -506,7 +784,13 @@ __device__ void run_query(const SeismicLaunch& a, const WarpSlice<V>& w, float* 
                     if (lane == 0) bscore[bb] = -INFINITY;
                     __syncwarp();
                     ++blocks_visited;
-                    visit_block<V>(a, w, lb0 + bb, n, lane, docs_scored, bytes, lane_bytes);
+                    if constexpr (kStaged) {
+                        ok = visit_block_staged<V>(a, w, lb0 + bb, n, lane, phase_bits, docs_scored,
+                                                   bytes, lane_bytes);
+                        if (!ok) break;
+                    } else {
+                        visit_block<V>(a, w, lb0 + bb, n, lane, docs_scored, bytes, lane_bytes);
+                    }
                 }
             } else {
                 for (int b0 = 0; b0 < nb; b0 += 32) {
@@ -521,13 +805,23 @@ __device__ void run_query(const SeismicLaunch& a, const WarpSlice<V>& w, float* 
                         const float S = __shfl_sync(kFull, s, src);
                         if (n == a.k && __fmul_rn(S, a.heap_factor) < w.hs[a.k - 1]) continue;
                         ++blocks_visited;
-                        visit_block<V>(a, w, lb0 + b0 + src, n, lane, docs_scored, bytes, lane_bytes);
+                        if constexpr (kStaged) {
+                            ok = visit_block_staged<V>(a, w, lb0 + b0 + src, n, lane, phase_bits,
+                                                       docs_scored, bytes, lane_bytes);
+                            if (!ok) break;
+                        } else {
+                            visit_block<V>(a, w, lb0 + b0 + src, n, lane, docs_scored, bytes,
+                                           lane_bytes);
+                        }
                     }
+                    if (!ok) break;
                 }
             }
         }
+        if (!ok) break;
         first = false;  // seismic_index.cpp:261
     }
+    if (!ok) n = 0;  // a gave-up wait leaves this query's results as padding
 
     // 6. results, padded with (-1.0, -1); SQ scores decoded
     //    (seismic_scalar_quantized_index.cpp:345-355).
@@ -553,29 +847,42 @@ __device__ void run_query(const SeismicLaunch& a, const WarpSlice<V>& w, float* 
         atomicAdd(a.stats + kStatListsProbed, lists);
     }
     __syncwarp();
+    return ok;
 }
 
-template <typename V>
+template <typename V, bool kStaged>
 __global__ void __launch_bounds__(256) seismic_search_kernel(SeismicLaunch a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const size_t per = slice_bytes(static_cast<int>(sizeof(V)), a.ix.words, a.qcap, a.k);
-    WarpSlice<V> w = carve<V>(smem + per * warp, a.ix.words, a.qcap, a.k);
+    const int bcap = kStaged ? a.bcap : 0;
+    const int sb = kStaged ? a.stage_bytes : 0;
+    const size_t per = slice_bytes(static_cast<int>(sizeof(V)), a.ix.words, a.qcap, a.k, bcap, sb);
+    WarpSlice<V> w = carve<V>(smem + per * warp, a.ix.words, a.qcap, a.k, bcap, sb);
     const int wpb = blockDim.x >> 5;
     const int gw = blockIdx.x * wpb + warp;
     float* bscore = a.bscore + static_cast<size_t>(gw) * a.ix.max_blocks;
+    uint32_t phase_bits = 0;
+    if constexpr (kStaged) {
+        if (lane == 0) {
+            mbar_init(w.mbar, 1);
+            mbar_init(w.mbar + 1, 1);
+            fence_mbar_init();
+        }
+        __syncwarp();
+    }
     if (a.work_counter != nullptr) {
         for (;;) {
             int q = 0;
             if (lane == 0) q = atomicAdd(a.work_counter, 1);
             q = __shfl_sync(kFull, q, 0);
             if (q >= a.q.n) break;
-            run_query<V>(a, w, bscore, q, lane);
+            if (!run_query<V, kStaged>(a, w, bscore, q, lane, phase_bits)) break;
         }
     } else {
         const int total = gridDim.x * wpb;
-        for (int q = a.first_query + gw; q < a.q.n; q += total) run_query<V>(a, w, bscore, q, lane);
+        for (int q = a.first_query + gw; q < a.q.n; q += total)
+            if (!run_query<V, kStaged>(a, w, bscore, q, lane, phase_bits)) break;
     }
 }
 
@@ -674,53 +981,64 @@ __global__ void sq_encode_kernel(const float* vals, void* codes, int64_t n, int 
 
 }  // namespace
 
-size_t seismic_smem_per_warp(int val_kind, int dim_words, int qcap, int k) {
-    return slice_bytes(val_kind, dim_words, qcap, k);
+size_t seismic_smem_per_warp(int val_kind, int dim_words, int qcap, int k, int bcap,
+                             int stage_bytes) {
+    return slice_bytes(val_kind, dim_words, qcap, k, bcap, stage_bytes);
 }
 
-int seismic_max_blocks_per_sm(int val_kind, int warps_per_block, size_t smem) {
-    int blocks = 0;
-    cudaError_t e = cudaSuccess;
+template <typename V, bool kStaged>
+static int max_blocks_typed(int wpb, size_t smem) {
     // the occupancy calculator only admits dynamic shared memory the kernel
     // has been allowed to use
-    if (val_kind == kF32)
-        e = cudaFuncSetAttribute(seismic_search_kernel<float>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    else if (val_kind == kU8)
-        e = cudaFuncSetAttribute(seismic_search_kernel<uint8_t>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    else
-        e = cudaFuncSetAttribute(seismic_search_kernel<uint16_t>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (e != cudaSuccess) return 0;
-    if (val_kind == kF32)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, seismic_search_kernel<float>,
-                                                          warps_per_block * 32, smem);
-    else if (val_kind == kU8)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, seismic_search_kernel<uint8_t>,
-                                                          warps_per_block * 32, smem);
-    else
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, seismic_search_kernel<uint16_t>,
-                                                          warps_per_block * 32, smem);
-    return e == cudaSuccess ? blocks : 0;
+    if (cudaFuncSetAttribute(seismic_search_kernel<V, kStaged>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem)) != cudaSuccess)
+        return 0;
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, seismic_search_kernel<V, kStaged>,
+                                                      wpb * 32, smem) != cudaSuccess)
+        return 0;
+    return blocks;
 }
 
-template <typename V>
+int seismic_max_blocks_per_sm(int val_kind, int variant, int wpb, size_t smem) {
+    if (val_kind == kF32)
+        return variant ? max_blocks_typed<float, true>(wpb, smem) : max_blocks_typed<float, false>(wpb, smem);
+    if (val_kind == kU8)
+        return variant ? max_blocks_typed<uint8_t, true>(wpb, smem)
+                       : max_blocks_typed<uint8_t, false>(wpb, smem);
+    return variant ? max_blocks_typed<uint16_t, true>(wpb, smem)
+                   : max_blocks_typed<uint16_t, false>(wpb, smem);
+}
+
+int seismic_max_blocks_per_sm(int val_kind, int wpb, size_t smem) {
+    return seismic_max_blocks_per_sm(val_kind, 0, wpb, smem);
+}
+
+template <typename V, bool kStaged>
 static cudaError_t launch_typed(const SeismicLaunch& a, int wpb, int blocks, cudaStream_t s) {
-    const size_t smem = slice_bytes(static_cast<int>(sizeof(V)), a.ix.words, a.qcap, a.k) * wpb;
-    cudaError_t e = cudaFuncSetAttribute(seismic_search_kernel<V>,
+    const size_t smem = slice_bytes(static_cast<int>(sizeof(V)), a.ix.words, a.qcap, a.k,
+                                    kStaged ? a.bcap : 0, kStaged ? a.stage_bytes : 0) *
+                        wpb;
+    cudaError_t e = cudaFuncSetAttribute(seismic_search_kernel<V, kStaged>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    seismic_search_kernel<V><<<blocks, wpb * 32, smem, s>>>(a);
+    seismic_search_kernel<V, kStaged><<<blocks, wpb * 32, smem, s>>>(a);
     return cudaGetLastError();
 }
 
 cudaError_t launch_seismic(int val_kind, const SeismicLaunch& a, int wpb, int blocks,
                            cudaStream_t s) {
-    if (val_kind == kF32) return launch_typed<float>(a, wpb, blocks, s);
-    if (val_kind == kU8) return launch_typed<uint8_t>(a, wpb, blocks, s);
-    return launch_typed<uint16_t>(a, wpb, blocks, s);
+    const bool staged = a.variant == 1 && a.stage_bytes > 0;
+    if (val_kind == kF32)
+        return staged ? launch_typed<float, true>(a, wpb, blocks, s)
+                      : launch_typed<float, false>(a, wpb, blocks, s);
+    if (val_kind == kU8)
+        return staged ? launch_typed<uint8_t, true>(a, wpb, blocks, s)
+                      : launch_typed<uint8_t, false>(a, wpb, blocks, s);
+    return staged ? launch_typed<uint16_t, true>(a, wpb, blocks, s)
+                  : launch_typed<uint16_t, false>(a, wpb, blocks, s);
 }
 
 template <typename V>

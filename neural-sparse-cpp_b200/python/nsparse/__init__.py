@@ -70,6 +70,7 @@ _sig("nsp_seismic_sq_search_params_new", ctypes.c_float, ctypes.c_float, ctypes.
      ctypes.c_float, ctypes.POINTER(_P))
 _sig("nsp_search_params_set_id_selector", _P, _P)
 _sig("nsp_search_params_set_engine", _P, ctypes.c_int, ctypes.c_int)
+_sig("nsp_search_params_set_kernel", _P, ctypes.c_int, ctypes.c_int)
 _sig("nsp_search_params_free", _P)
 _sig("nsp_index_search_device", _P, _I32, _P, _P, _P, _I32, ctypes.c_int, _P, _P, _P, _P)
 _sig("nsp_device_info", ctypes.POINTER(_I32), ctypes.c_char_p, ctypes.c_size_t)
@@ -184,6 +185,11 @@ class SearchParameters:
     def set_engine(self, plain=False, warps_per_block=0):
         """Extension: plain=True runs one kernel launch per query."""
         _check(_L.nsp_search_params_set_engine(self._h, int(bool(plain)), int(warps_per_block)))
+
+    def set_kernel(self, variant=-1, stage_bytes=0):
+        """Extension: SEISMIC kernel variant (-1 auto, 0 direct loads, 1 bulk-copy
+        staging) and staging buffer bytes. Results do not depend on either."""
+        _check(_L.nsp_search_params_set_kernel(self._h, int(variant), int(stage_bytes)))
 
     def __del__(self):
         h, self._h = getattr(self, "_h", None), None

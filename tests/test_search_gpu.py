@@ -163,6 +163,37 @@ def test_seismic_plain_equals_batched(seismic_file):
         np.testing.assert_array_equal(Dw, Db)
 
 
+@pytest.mark.parametrize("variant,stage", [(0, 0), (1, 0), (1, 2048), (1, 128)])
+@pytest.mark.parametrize("kind", ["fp32", "sq8"])
+def test_seismic_kernel_variants_agree(tmp_path, variant, stage, kind):
+    """Direct row loads, bulk-copy staging, and staging buffers so small that
+    most rows are scored from HBM in their place: identical results."""
+    docs, qs = golden_corpus()
+    spec = SEISMIC if kind == "fp32" else sq_spec(float(docs.values.min()),
+                                                  float(docs.values.max()))
+    ref_file(docs, spec, tmp_path / "v.idx")
+    idx = nsparse.read_index(str(tmp_path / "v.idx"))
+    base = nsparse.SeismicSearchParameters(CUT, HF)
+    base.set_kernel(0, 0)
+    D0, L0 = search(idx, qs, params=base)
+    p = nsparse.SeismicSearchParameters(CUT, HF)
+    p.set_kernel(variant, stage)
+    D, L = search(idx, qs, params=p)
+    np.testing.assert_array_equal(L, L0)
+    np.testing.assert_array_equal(D, D0)
+    p.set_engine(plain=True)
+    Dp, Lp = search(idx, qs.rows(0, 8), params=p)
+    np.testing.assert_array_equal(Lp, L0[:8])
+    sel = nsparse.SetIDSelector(np.arange(0, docs.n, 3, dtype=np.int32))
+    p2 = nsparse.SeismicSearchParameters(CUT, HF)
+    p2.set_kernel(variant, stage)
+    p2.set_id_selector(sel)
+    b2 = nsparse.SeismicSearchParameters(CUT, HF)
+    b2.set_kernel(0, 0)
+    b2.set_id_selector(sel)
+    np.testing.assert_array_equal(search(idx, qs, params=p2)[1], search(idx, qs, params=b2)[1])
+
+
 def test_seismic_filter_and_exact_path_match_golden(seismic_file):
     g = golden()
     _, qs = golden_corpus()
