@@ -32,7 +32,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstdint>
 #include <cstring>
 #include <random>
@@ -673,6 +676,26 @@ void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
     }
 }
 
+// Phase timings on stderr when NSP_VERBOSE=1 (the engine's one debug switch).
+struct PhaseClock {
+    cudaStream_t s;
+    bool on;
+    std::chrono::steady_clock::time_point t;
+    explicit PhaseClock(cudaStream_t st) : s(st) {
+        const char* v = std::getenv("NSP_VERBOSE");
+        on = v != nullptr && v[0] == '1';
+        t = std::chrono::steady_clock::now();
+    }
+    void mark(const char* what) {
+        if (!on) return;
+        cudaStreamSynchronize(s);
+        const auto now = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "[nsparse build] %-12s %8.3f s\n", what,
+                     std::chrono::duration<double>(now - t).count());
+        t = now;
+    }
+};
+
 template <int ESZ>
 void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
     const nsp::HostCsr& h = st.vectors.host;
@@ -687,6 +710,7 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
     const nsp::FwdView f = st.vectors.dev.view();
     const int32_t n_lists = dim;
     const int sms = nsp::device_sm_count();
+    PhaseClock clock(s);
 
     // ---- 1. postings
     DevArray<unsigned long long> cnt(static_cast<size_t>(n_lists) + 1);
@@ -726,6 +750,7 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
     cuda_check(cudaStreamSynchronize(s), "sync");
     keys2.reset();
 
+    clock.mark("postings");
     // ---- 2. centroid positions (host; depends on list lengths only)
     std::vector<int64_t> cptr(n_lists + 1, 0);
     for (int32_t t = 0; t < n_lists; ++t)
@@ -760,6 +785,7 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
     to_dev(d_cptr, cptr, s);
     to_dev(d_cpos, cpos, s);
 
+    clock.mark("centroids");
     // ---- 3. assignment
     DevArray<uint32_t> akey(static_cast<size_t>(std::max<int64_t>(total_kept, 1)));
     if (total_kept > 0) {
@@ -804,6 +830,7 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
         cuda_check(cudaStreamSynchronize(s), "assign sync");
     }
 
+    clock.mark("assignment");
     // ---- 4. blocks: centroid first, members in list order
     DevArray<int32_t> bdocs(static_cast<size_t>(std::max<int64_t>(total_kept, 1)));
     DevArray<uint32_t> akey2(static_cast<size_t>(std::max<int64_t>(total_kept, 1)));
@@ -833,6 +860,7 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
     }
     const int64_t n_blocks = L.lbp.back();
 
+    clock.mark("blocks");
     // ---- 5. summaries, in batches of lists bounded by entry count
     std::vector<int64_t> doc_len(static_cast<size_t>(total_kept));
     for (int64_t j = 0; j < total_kept; ++j) {
@@ -869,6 +897,7 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
         t0 = t1;
     }
 
+    clock.mark("summaries");
     // ---- 6. publish
     std::lock_guard<std::mutex> g(st.mu);
     st.lists = std::move(L);
