@@ -15,6 +15,9 @@ queries, search, D2H of the results). The index (~5 GB) exceeds L2, and L2 is
 also flushed between timed steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+  python bench.py --docs 300000 --queries 4000 --kernel-only --variant 2
+      (a smaller case of the same workload, search launches only: the
+      profiling case; --variant/--tuning pick the search kernel)
 
 Under torchrun each rank is a replica holding the whole index and searching
 its own 10,000 queries (weak scaling, no collective on the data path).
@@ -227,6 +230,7 @@ def run_engine(args):
     build_s = time.perf_counter() - t
     log(f"rank {rank}: device build {build_s:.1f}s")
     params = nsparse.SeismicSearchParameters(CUT, HF)
+    params.set_kernel(args.variant, args.tuning)
 
     # ---- device-resident inputs and outputs
     d_ip = torch.from_numpy(qs.indptr).to(dev)
@@ -263,6 +267,13 @@ def run_engine(args):
         torch.cuda.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = sum(step_ms)
+    if args.kernel_only:
+        if rank == 0:
+            print(json.dumps({"case": dict(WORKLOAD, docs=docs.n, queries=qs.n),
+                              "variant": args.variant, "tuning": args.tuning,
+                              "ms_per_step": total_ms / args.steps,
+                              "queries_per_s": qs.n * args.steps / (total_ms / 1000.0)}))
+        return
     # kernel-only time and algorithmic bytes of one batched search (engine stats)
     D, L = idx.search(qs.n, qs.indptr, qs.indices, qs.values, K, params)
     st = nsparse.last_search_stats()
@@ -334,7 +345,9 @@ def run_engine(args):
             "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": my_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": dict(WORKLOAD, parallelism=f"replicas{world}"),
+            "data": "synthetic", "config": dict(WORKLOAD, parallelism=f"replicas{world}",
+                                                kernel_variant=args.variant,
+                                                kernel_tuning=args.tuning),
             "recall_at_10": rec, "build_s": build_s,
             "plain": {"qps": plain_qps, "queries": n_plain,
                       "p50_ms": lat_ms[len(lat_ms) // 2], "p99_ms": lat_ms[int(0.99 * (len(lat_ms) - 1))],
@@ -359,13 +372,24 @@ def run_engine(args):
 
 
 def main():
+    global N_DOCS, N_QUERIES
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--docs", type=int, default=N_DOCS, help="corpus size (default: the workload's)")
+    ap.add_argument("--queries", type=int, default=N_QUERIES)
+    ap.add_argument("--variant", type=int, default=-1, help="search kernel (-1: engine's choice)")
+    ap.add_argument("--tuning", type=int, default=0, help="the kernel's tuning value (0: default)")
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="time the device-resident search launches only and exit")
     args = ap.parse_args()
+    if (args.docs, args.queries) != (N_DOCS, N_QUERIES):
+        N_DOCS, N_QUERIES = args.docs, args.queries
+        WORKLOAD.update(workload=f"seismic_fp32_{N_DOCS}_docs_{N_QUERIES}_queries", docs=N_DOCS,
+                        queries=N_QUERIES)
     if args.impl == "reference":
         run_reference(args)
     else:

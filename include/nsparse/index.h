@@ -20,11 +20,14 @@ namespace nsparse {
 struct EngineOptions {
     bool plain = false;
     int warps_per_block = 0;
-    // SEISMIC kernel variant: -1 lets the engine choose, 0 loads doc rows
-    // straight from HBM, 1 stages them in shared memory by bulk copy
-    // (stage_bytes per buffer, 0 = default). Results are identical.
+    // SEISMIC kernel variant: -1 lets the engine choose, 0 one warp per query
+    // loading doc rows straight from HBM, 1 the same with rows staged in
+    // shared memory by bulk copy (stage_bytes per buffer, 0 = default), 2-4
+    // one CTA per query with 1, 2 or 4 lanes per scored doc, in batches of
+    // batch_docs candidate docs (0 = default). Results are identical.
     int variant = -1;
     int stage_bytes = 0;
+    int batch_docs = 0;
 };
 
 struct SearchParameters {

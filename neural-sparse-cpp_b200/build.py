@@ -52,7 +52,7 @@ def _stale(target, sources):
 
 
 def _headers():
-    return (glob.glob(os.path.join(CSRC, "*.h")) +
+    return (glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) +
             glob.glob(os.path.join(ROOT, "include", "**", "*.h"), recursive=True))
 
 

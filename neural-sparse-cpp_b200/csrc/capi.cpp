@@ -238,14 +238,23 @@ nsp_status_t nsp_search_params_set_engine(nsp_search_params_t* params, int plain
 }
 
 nsp_status_t nsp_search_params_set_kernel(nsp_search_params_t* params, int variant,
-                                          int stage_bytes) {
+                                          int tuning) {
     return guarded([&] {
         if (params == nullptr) throw std::invalid_argument("unexpected nullptr");
-        if (variant < -1 || variant > 1) throw std::invalid_argument("variant must be -1, 0 or 1");
-        if (stage_bytes < 0 || stage_bytes > (96 << 10))
-            throw std::invalid_argument("stage_bytes must be in [0, 98304]");
-        as_params(params)->engine.variant = variant;
-        as_params(params)->engine.stage_bytes = stage_bytes;
+        if (variant < -1 || variant > 4) throw std::invalid_argument("variant must be in [-1, 4]");
+        auto& e = as_params(params)->engine;
+        e.variant = variant;
+        e.stage_bytes = 0;
+        e.batch_docs = 0;
+        if (variant >= 2) {
+            if (tuning < 0 || tuning > 8192)
+                throw std::invalid_argument("batch_docs must be in [0, 8192]");
+            e.batch_docs = tuning;
+        } else {
+            if (tuning < 0 || tuning > (96 << 10))
+                throw std::invalid_argument("stage_bytes must be in [0, 98304]");
+            e.stage_bytes = tuning;
+        }
     });
 }
 

@@ -80,7 +80,7 @@ class Workspace {
 public:
     enum Slot : int {
         kQIndptr, kQIdx, kQVal, kQCode, kOutD, kOutL, kSel, kBScore, kCounter, kStats,
-        kCandD, kCandL, kHeapD, kHeapL, kQValG, kIds, kErr, kNumSlots
+        kCandD, kCandL, kHeapD, kHeapL, kQValG, kIds, kErr, kOrder, kSortKeys, kNumSlots
     };
     static Workspace& get();
     cudaStream_t stream() const { return stream_; }
@@ -205,8 +205,10 @@ struct SeismicSearchArgs {
     float decode_scale = 0.0f;
     bool plain = false;       // one query per launch
     int warps_per_block = 0;  // 0 = autotuned
-    int variant = -1;         // -1 auto, 0 direct row loads, 1 bulk-copy staged rows
+    int variant = -1;         // -1 auto, 0 direct row loads, 1 bulk-copy staged rows,
+                              // 2-4 one CTA per query with 1, 2, 4 lanes per doc
     int stage_bytes = 0;      // staged: bytes per stage buffer (0 = default)
+    int batch_docs = 0;       // variants 2-4: candidate docs per batch (0 = default)
 };
 
 // Host buffers in, host buffers out (the reference-facing path).

@@ -77,6 +77,7 @@ nsp::SeismicSearchArgs seismic_args(const SearchParameters* p, int k) {
         a.warps_per_block = p->engine.warps_per_block;
         a.variant = p->engine.variant;
         a.stage_bytes = p->engine.stage_bytes;
+        a.batch_docs = p->engine.batch_docs;
     }
     return a;
 }

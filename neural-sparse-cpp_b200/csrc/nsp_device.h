@@ -97,7 +97,18 @@ struct SeismicLaunch {
     int32_t variant;
     int32_t stage_bytes;
     int32_t bcap;
-    int32_t* err;               // set to 1 when a bounded wait gives up
+    int32_t* err;               // nonzero: a kernel-side error (see check_kernel_error)
+    // Variants 2-4 (one CTA per query): candidate docs per batch, lanes per
+    // scored doc (1, 2, 4), and per-CTA scratch -- `bscore` holds warps *
+    // max_blocks floats per CTA, `order` the first list's visiting order,
+    // `sortkeys` the sort buffer of lists too long to sort in shared memory
+    // (nullptr when none is).
+    int32_t batch_docs;
+    int32_t group_lanes;
+    uint16_t* order;
+    int32_t order_stride;
+    unsigned long long* sortkeys;
+    int32_t sort_stride;
 };
 
 struct ExactLaunch {
@@ -126,6 +137,13 @@ cudaError_t launch_seismic(int val_kind, const SeismicLaunch& a, int warps_per_b
                            int blocks, cudaStream_t s);
 int seismic_max_blocks_per_sm(int val_kind, int variant, int warps_per_block, size_t smem);
 int seismic_max_blocks_per_sm(int val_kind, int warps_per_block, size_t smem);  // variant 0
+
+// Variants 2-4: one CTA of `warps` warps per query (search_seismic_cta.cu).
+size_t seismic_cta_smem(int val_kind, int dim, int qcap, int k, int batch_docs);
+int seismic_cta_max_blocks_per_sm(int val_kind, int qcap, int group_lanes, int warps,
+                                  size_t smem);
+cudaError_t launch_seismic_cta(int val_kind, const SeismicLaunch& a, int warps, int blocks,
+                               cudaStream_t s);
 
 size_t exact_smem(int dim_words, int qcap_smem);  // qcap_smem 0: values in global
 cudaError_t launch_exact(const ExactLaunch& a, int tiles, cudaStream_t s);

@@ -1,0 +1,877 @@
+// SEISMIC / SEISMIC-SQ search on sm_100a, one CTA per query (kernel
+// variants 2-4). A persistent grid steals queries from a global counter; the
+// CTA's warps walk the query's blocks together.
+//
+// Per query (seismic_index.cpp:231-274, seismic_scalar_quantized_index.cpp:
+// 307-357):
+//   1. the query is scattered into a dense per-term table in shared memory --
+//      the reference's dimension-sized dense buffer (seismic_index.cpp:243-
+//      246), one byte per term: fp32 queries store the term's rank (0 = not
+//      in the query; the rank indexes a table of the query's values, entry 0
+//      holding 0.0f), SQ queries store the code itself;
+//   2. the query cut (utils/vector_process.h:18-30) is a rank selection;
+//   3. block summary scores (inverted_list_clusters.cpp:295-331) of up to
+//      one list per warp are accumulated at once, each warp hit term by hit
+//      term in ascending term order;
+//   4. the first list's blocks are sorted (score desc, block asc) by a
+//      bitonic sort (seismic_common.h:105-115); later lists keep block order;
+//   5. blocks are taken in that order into batches of up to `batch_docs`
+//      docs. A block that fails the pruning test (seismic_index.cpp:78-86)
+//      against the current heap minimum is skipped (or ends the first list);
+//      the heap minimum only grows, so a block that fails now fails at its
+//      turn too. Blocks that pass are gathered, their docs scored in
+//      parallel, and then -- in block order -- each block is tested again
+//      against the heap as it stands when its turn comes, exactly as the
+//      reference tests it, and its docs are offered in order. Docs of a block
+//      that fails the second test are dropped: the result is the reference's,
+//      only some scoring work is speculative;
+//   6. a group of kG lanes (1, 2 or 4) scores one doc at a time, 16 row
+//      elements per lane per step from 256-bit loads of the padded forward
+//      rows, and takes the next doc of the batch as soon as its row ends, so
+//      groups stay busy across rows of different lengths. fp32 scores are the
+//      reference's sequential sum result += w * dense[t] over the whole row
+//      (utils/distance.h:29-37), with the same round-to-nearest products and
+//      sums in the same order: bit-identical. The zero padding after a row
+//      adds +-0.0, which leaves every sum unchanged unless the query holds a
+//      non-finite value, in which case padding elements are masked out. SQ
+//      sums are exact integers (distance.h:39-57);
+//   7. scores enter a shared-memory top-k in the reference's insertion order;
+//      a doc already in the heap is skipped and one scored before and
+//      evicted or rejected scores <= the (monotone) heap minimum and is
+//      rejected again: the reference's visited set (seismic_index.cpp:104-
+//      107) without an O(n_docs) bitmap per query.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <climits>
+#include <cstdint>
+#include <type_traits>
+
+#include "nsp_device.h"
+#include "search_common.cuh"
+
+namespace nsp {
+namespace {
+
+using detail_search::heap_offer;
+using detail_search::kFull;
+using detail_search::ValT;
+
+constexpr int kSegCap = 128;  // block segments per batch
+
+// A run of consecutive docs of one block inside a batch.
+struct Seg {
+    int64_t d0;     // position of the first doc in ix.docs
+    int32_t cnt;    // docs in the segment
+    int32_t cand0;  // first candidate slot of the batch
+    int32_t blk;    // block index within its list
+    float bs;       // the block's summary score
+    int32_t head;   // 1 when the block starts here (its pruning test applies)
+    int32_t pad;
+};
+
+struct Ctl {
+    int32_t q;
+    int32_t nseg;
+    int32_t total;
+    int32_t next;  // claim counter of the scoring phase
+    int32_t pad[4];
+};
+
+__host__ __device__ inline size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
+
+struct CtaLayout {
+    size_t tbl, qv, qterm, qraw, cuts, hs, hid, cdoc, coff, clen, csc, segs, total;
+};
+
+// Shared-memory layout of one CTA. The four candidate arrays are contiguous
+// (16 * batch bytes) and double as the sort-key buffer of the first list.
+__host__ __device__ inline CtaLayout cta_layout(int vsize, int tsize, int dim, int qcap, int k,
+                                                int batch) {
+    CtaLayout L;
+    size_t o = a16(sizeof(Ctl));
+    L.tbl = o;   o += a16(static_cast<size_t>(dim + 1) * tsize);
+    L.qv = o;    o += a16(static_cast<size_t>(qcap + 1) * 4);
+    L.qterm = o; o += a16(static_cast<size_t>(qcap) * 2);
+    L.qraw = o;  o += a16(static_cast<size_t>(qcap) * vsize);
+    L.cuts = o;  o += a16(static_cast<size_t>(qcap) * 2);
+    L.hs = o;    o += a16(static_cast<size_t>(k) * 4);
+    L.hid = o;   o += a16(static_cast<size_t>(k) * 4);
+    L.cdoc = o;  o += static_cast<size_t>(batch) * 4;
+    L.coff = o;  o += static_cast<size_t>(batch) * 4;
+    L.clen = o;  o += static_cast<size_t>(batch) * 4;
+    L.csc = o;   o += static_cast<size_t>(batch) * 4;
+    L.segs = o;  o += static_cast<size_t>(kSegCap) * sizeof(Seg);
+    L.total = o;
+    return L;
+}
+
+// ------------------------------------------------------------ row loads --
+// 256-bit loads (sm_100): a lane reads 16 term ids (32 bytes) per step and
+// their values (64 bytes fp32, 32 bytes uint16, 16 bytes uint8).
+__device__ __forceinline__ void ldg256(const void* p, uint32_t (&r)[8]) {
+    asm("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7])
+        : "l"(p));
+}
+
+__device__ __forceinline__ uint32_t term_of(const uint32_t (&t)[8], int u) {
+    return (u & 1) ? (t[u >> 1] >> 16) : (t[u >> 1] & 0xffffu);
+}
+
+template <typename V>
+struct Acc;
+template <>
+struct Acc<float> {
+    using T = float;
+};
+template <>
+struct Acc<uint8_t> {
+    using T = int;
+};
+template <>
+struct Acc<uint16_t> {
+    using T = long long;
+};
+
+// Products of one lane's 16 row elements at ip/vp, `rem` of them real (the
+// rest are the row's zero padding, or nothing when rem <= 0).
+// fp32: p[u] = w[u] * qv[tbl[t[u]]], the reference's product; with kMask the
+// padding gives +0.0.
+template <typename TE, bool kMask>
+__device__ __forceinline__ void products(const uint16_t* ip, const float* vp, int rem,
+                                         const TE* tbl, const float* qv, float (&p)[16]) {
+    if (rem <= 0) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) p[u] = 0.0f;
+        return;
+    }
+    uint32_t t[8], v0[8], v1[8];
+    ldg256(ip, t);
+    ldg256(vp, v0);
+    ldg256(vp + 8, v1);
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+        const float q = qv[tbl[term_of(t, u)]];
+        const float x = __uint_as_float(u < 8 ? v0[u] : v1[u - 8]);
+        p[u] = __fmul_rn(x, q);
+        if (kMask && u >= rem) p[u] = 0.0f;
+    }
+}
+
+// uint8 codes: the sum of code products as int (distance.h:39-47); padding
+// codes are 0.
+template <typename TE>
+__device__ __forceinline__ int partial(const uint16_t* ip, const uint8_t* vp, int rem,
+                                       const TE* tbl) {
+    if (rem <= 0) return 0;
+    uint32_t t[8];
+    ldg256(ip, t);
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(vp));
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+    int acc = 0;
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+        const int q = static_cast<int>(tbl[term_of(t, u)]);
+        const int x = static_cast<int>((w[u >> 2] >> (8 * (u & 3))) & 0xffu);
+        acc += x * q;
+    }
+    return acc;
+}
+
+// uint16 codes: int64 sum (distance.h:49-57).
+template <typename TE>
+__device__ __forceinline__ long long partial(const uint16_t* ip, const uint16_t* vp, int rem,
+                                             const TE* tbl) {
+    if (rem <= 0) return 0;
+    uint32_t t[8], v[8];
+    ldg256(ip, t);
+    ldg256(vp, v);
+    long long acc = 0;
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+        const unsigned long long q = static_cast<unsigned long long>(tbl[term_of(t, u)]);
+        const unsigned long long x = static_cast<unsigned long long>(term_of(v, u));
+        acc += static_cast<long long>(x * q);
+    }
+    return acc;
+}
+
+// fp32: folds the group's products into acc in row order -- lane 0's 16,
+// then lane 1's, ... -- one FADD per product, the reference's sequence of
+// roundings. Every lane of the warp takes part (the shuffles are warp-wide);
+// `acc` is the same on every lane of a group and comes back the same.
+template <int kG>
+__device__ __forceinline__ float fold(float acc, const float (&p)[16], int gbase) {
+    if constexpr (kG == 1) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) acc = __fadd_rn(acc, p[u]);
+        return acc;
+    } else {
+        float a = acc;
+#pragma unroll
+        for (int l = 0; l < kG; ++l) {
+            float r = a;
+#pragma unroll
+            for (int u = 0; u < 16; ++u) r = __fadd_rn(r, p[u]);
+            a = __shfl_sync(kFull, r, gbase + l);
+        }
+        return a;
+    }
+}
+
+// Integer partial sums of a group, exact in any order.
+template <int kG, typename A>
+__device__ __forceinline__ A group_sum(A x) {
+#pragma unroll
+    for (int o = kG / 2; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+    return x;
+}
+
+__device__ __forceinline__ float finish(float a) { return a; }
+__device__ __forceinline__ float finish(int a) { return static_cast<float>(a); }
+__device__ __forceinline__ float finish(long long a) { return static_cast<float>(a); }
+
+// Scoring phase. Lanes work in groups of kG (aligned within the warp); a
+// group claims one candidate of the batch at a time and walks its row kG*16
+// elements per step, lane l of the group taking elements 16l..16l+15 of the
+// step, so a step's loads are kG*32 contiguous bytes of ids and the matching
+// contiguous values. A group whose row ends takes the next candidate at the
+// following step.
+template <typename V, typename TE, bool kMask, int kG>
+__device__ void score_batch(const FwdView& fwd, Ctl* ctl, const TE* tbl, const float* qv,
+                            const uint32_t* coff, const uint32_t* clen, float* csc, int total,
+                            int lane) {
+    using A = typename Acc<V>::T;
+    constexpr bool kF32 = std::is_same<V, float>::value;
+    const uint16_t* idx_base = fwd.idx;
+    const V* val_base = static_cast<const V*>(fwd.val);
+    const int gl = lane & (kG - 1);
+    const int gbase = lane - gl;
+    int i = -1;  // the group's candidate (the same on every lane of the group)
+    const uint16_t* ip = nullptr;
+    const V* vp = nullptr;
+    int rem = 0;  // row elements from this step on
+    A acc = 0;
+    bool fin = false;
+    for (;;) {
+        const bool want = !fin && i < 0;
+        const unsigned wm = __ballot_sync(kFull, want && gl == 0);
+        if (wm) {
+            const int leader = __ffs(wm) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(&ctl->next, __popc(wm));
+            base = __shfl_sync(kFull, base, leader);
+            if (want) {
+                const int j = base + __popc(wm & ((1u << gbase) - 1u));
+                if (j < total) {
+                    i = j;
+                    const size_t e0 = static_cast<size_t>(coff[j]) * kRowAlign + 16 * gl;
+                    ip = idx_base + e0;
+                    vp = val_base + e0;
+                    rem = static_cast<int>(clen[j]);
+                    acc = 0;
+                } else {
+                    fin = true;
+                }
+            }
+        }
+        const bool act = i >= 0;
+        if (!__any_sync(kFull, act)) break;
+        const int mine = act ? rem - 16 * gl : 0;  // this lane's real elements
+        if constexpr (kF32) {
+            float p[16];
+            products<TE, kMask>(ip, vp, mine, tbl, qv, p);
+            acc = fold<kG>(acc, p, gbase);
+        } else {
+            acc += group_sum<kG>(partial<TE>(ip, vp, mine, tbl));
+        }
+        if (act) {
+            ip += 16 * kG;
+            vp += 16 * kG;
+            rem -= 16 * kG;
+            if (rem <= 0) {
+                if (gl == 0) csc[i] = finish(acc);
+                i = -1;
+            }
+        }
+    }
+}
+
+// Summary scores of list t into bscore[0..nb): hit terms in ascending term
+// order, lanes spread over the term's (block, value) run.
+template <typename V>
+__device__ void list_summaries(const SeismicLaunch& a, int t, int nb, const uint16_t* qterm,
+                               const V* qraw, int qn, float* bscore, int lane,
+                               unsigned long long& bytes) {
+    constexpr int vsz = static_cast<int>(sizeof(V));
+    for (int b = lane; b < nb; b += 32) bscore[b] = 0.0f;
+    __syncwarp();
+    const uint2* meta = a.ix.lmeta + static_cast<size_t>(t) * a.ix.words;
+    const int64_t colbase = a.ix.ltp[t];
+    for (int i0 = 0; i0 < qn; i0 += 32) {
+        const int i = i0 + lane;
+        bool hit = false;
+        int64_t r0 = 0, r1 = 0;
+        float qv = 0.0f;
+        if (i < qn && qterm[i] < static_cast<uint32_t>(a.fwd.dim)) {
+            const uint32_t term = qterm[i];
+            const uint2 m = __ldg(meta + (term >> 5));
+            const uint32_t bit = 1u << (term & 31);
+            if (m.x & bit) {
+                const int64_t col = colbase + m.y + __popc(m.x & (bit - 1));
+                r0 = __ldg(a.ix.srun + col);
+                r1 = __ldg(a.ix.srun + col + 1);
+                qv = ValT<V>::f(qraw[i]);
+                hit = true;
+            }
+        }
+        bytes += 8ull * static_cast<unsigned long long>(min(32, qn - i0));
+        unsigned hm = __ballot_sync(kFull, hit);
+        bytes += 16ull * __popc(hm);
+        while (hm) {
+            const int src = __ffs(hm) - 1;
+            hm &= hm - 1;
+            const int64_t R0 = __shfl_sync(kFull, r0, src);
+            const int64_t R1 = __shfl_sync(kFull, r1, src);
+            const float QV = __shfl_sync(kFull, qv, src);
+            bytes += static_cast<unsigned long long>(R1 - R0) * (2 + vsz);
+            const V* sv = static_cast<const V*>(a.ix.sval);
+            for (int64_t e = R0 + lane; e < R1; e += 32) {
+                const int blk = __ldg(a.ix.sblk + e);
+                const float p = __fmul_rn(QV, ValT<V>::f(__ldg(sv + e)));
+                bscore[blk] = __fadd_rn(bscore[blk], p);
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Sort key: ascending key order = score descending, block ascending. +0.0
+// and -0.0 compare equal, as the reference's comparator has them.
+__device__ __forceinline__ unsigned long long order_key(float s, int b) {
+    uint32_t u = __float_as_uint(s == 0.0f ? 0.0f : s);
+    u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);  // ascending with s
+    return (static_cast<unsigned long long>(~u) << 32) | static_cast<uint32_t>(b);
+}
+
+// Bitonic sort of the first list's blocks; writes the visiting order.
+__device__ void sort_blocks(const float* bscore, int nb, unsigned long long* keys, int p2,
+                            uint16_t* order, int tid, int nthreads) {
+    for (int i = tid; i < p2; i += nthreads)
+        keys[i] = i < nb ? order_key(bscore[i], i) : ~0ull;
+    __syncthreads();
+    for (int k2 = 2; k2 <= p2; k2 <<= 1) {
+        for (int j = k2 >> 1; j > 0; j >>= 1) {
+            for (int i = tid; i < p2; i += nthreads) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const unsigned long long x = keys[i];
+                    const unsigned long long y = keys[ixj];
+                    const bool up = (i & k2) == 0;
+                    if ((x > y) == up) {
+                        keys[i] = y;
+                        keys[ixj] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int i = tid; i < nb; i += nthreads) order[i] = static_cast<uint16_t>(keys[i] & 0xffffu);
+    __syncthreads();
+}
+
+// Cursor of warp 0 over one list's visiting order.
+struct Cursor {
+    int o;            // next position in the visiting order
+    bool dead;        // the first list's walk has ended
+    bool split;       // a block is part-way through
+    int64_t split_d;  // its next doc position
+    int split_left;
+    int split_blk;
+    float split_bs;
+};
+
+// Warp 0: fills the next batch with segments of blocks that pass the pruning
+// test against the current heap. Returns the number of segments; `total`
+// receives the number of docs.
+__device__ int gather(const SeismicLaunch& a, Cursor& c, bool first, int64_t lb0, int nb,
+                      const float* bscore, const uint16_t* order, int n, const float* hs,
+                      Seg* segs, int batch, int& total, int lane) {
+    int room = batch;
+    int nseg = 0;
+    total = 0;
+    if (c.split) {
+        const int take = min(room, c.split_left);
+        if (lane == 0) {
+            Seg g;
+            g.d0 = c.split_d;
+            g.cnt = take;
+            g.cand0 = 0;
+            g.blk = c.split_blk;
+            g.bs = c.split_bs;
+            g.head = 0;
+            g.pad = 0;
+            segs[0] = g;
+        }
+        nseg = 1;
+        total = take;
+        room -= take;
+        c.split_d += take;
+        c.split_left -= take;
+        if (c.split_left == 0) c.split = false;
+    }
+    const bool full = n == a.k;
+    const float hmin = full ? hs[a.k - 1] : 0.0f;
+    while (!c.split && !c.dead && room > 0 && nseg < kSegCap && c.o < nb) {
+        const int p = c.o + lane;
+        const bool in = p < nb;
+        int blk = 0;
+        float bs = 0.0f;
+        if (in) {
+            blk = first ? static_cast<int>(order[p]) : p;
+            bs = bscore[blk];
+        }
+        const bool pass = in && !(full && __fmul_rn(bs, a.heap_factor) < hmin);
+        const unsigned inm = __ballot_sync(kFull, in);
+        const unsigned pm = __ballot_sync(kFull, pass);
+        int lim = __popc(inm);
+        bool brk = false;
+        if (first) {
+            const unsigned fm = inm & ~pm;
+            if (fm) {
+                lim = __ffs(fm) - 1;
+                brk = true;
+            }
+        }
+        const bool cand = pass && lane < lim;
+        int64_t d0 = 0;
+        int sz = 0;
+        if (cand) {
+            d0 = __ldg(a.ix.bdp + lb0 + blk);
+            sz = static_cast<int>(__ldg(a.ix.bdp + lb0 + blk + 1) - d0);
+        }
+        int incl = sz;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int excl = incl - sz;
+        const unsigned cm = __ballot_sync(kFull, cand);
+        const int r = __popc(cm & ((1u << lane) - 1u));
+        const bool take = cand && excl < room && nseg + r < kSegCap;
+        const unsigned tm = __ballot_sync(kFull, take);
+        if (take) {
+            Seg g;
+            g.d0 = d0;
+            g.cnt = min(sz, room - excl);
+            g.cand0 = total + excl;
+            g.blk = blk;
+            g.bs = bs;
+            g.head = 1;
+            g.pad = 0;
+            segs[nseg + r] = g;
+        }
+        int taken_docs = 0;
+        if (tm) {
+            const int last = 31 - __clz(tm);
+            const int lsz = __shfl_sync(kFull, sz, last);
+            const int lexcl = __shfl_sync(kFull, excl, last);
+            const int lcnt = min(lsz, room - lexcl);
+            const int64_t ld0 = __shfl_sync(kFull, d0, last);
+            const int lblk = __shfl_sync(kFull, blk, last);
+            const float lbs = __shfl_sync(kFull, bs, last);
+            taken_docs = lexcl + lcnt;
+            if (lcnt < lsz) {
+                c.split = true;
+                c.split_d = ld0 + lcnt;
+                c.split_left = lsz - lcnt;
+                c.split_blk = lblk;
+                c.split_bs = lbs;
+            }
+        }
+        const unsigned nt = cm & ~tm;  // candidates left for the next batch
+        if (nt) {
+            c.o += __ffs(nt) - 1;
+        } else {
+            c.o += lim;
+            // the failing block ends the first list once the blocks before it
+            // (including a block cut short) are done
+            if (brk && !c.split) c.dead = true;
+        }
+        nseg += __popc(tm);
+        total += taken_docs;
+        room -= taken_docs;
+    }
+    __syncwarp();
+    return nseg;
+}
+
+template <typename V, typename TE, int kG>
+__global__ void __launch_bounds__(256, 4) seismic_cta_kernel(SeismicLaunch a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr bool kRank = std::is_same<V, float>::value;
+    constexpr int vsz = static_cast<int>(sizeof(V));
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int nwarps = blockDim.x >> 5;
+    const int dim = a.fwd.dim;
+    const int batch = a.batch_docs;
+    const CtaLayout L = cta_layout(vsz, static_cast<int>(sizeof(TE)), dim, a.qcap, a.k, batch);
+    Ctl* ctl = reinterpret_cast<Ctl*>(smem);
+    TE* tbl = reinterpret_cast<TE*>(smem + L.tbl);
+    float* qv = reinterpret_cast<float*>(smem + L.qv);
+    uint16_t* qterm = reinterpret_cast<uint16_t*>(smem + L.qterm);
+    V* qraw = reinterpret_cast<V*>(smem + L.qraw);
+    uint16_t* cuts = reinterpret_cast<uint16_t*>(smem + L.cuts);
+    float* hs = reinterpret_cast<float*>(smem + L.hs);
+    int32_t* hid = reinterpret_cast<int32_t*>(smem + L.hid);
+    int32_t* cdoc = reinterpret_cast<int32_t*>(smem + L.cdoc);
+    uint32_t* coff = reinterpret_cast<uint32_t*>(smem + L.coff);
+    uint32_t* clen = reinterpret_cast<uint32_t*>(smem + L.clen);
+    float* csc = reinterpret_cast<float*>(smem + L.csc);
+    Seg* segs = reinterpret_cast<Seg*>(smem + L.segs);
+
+    const int maxb = a.ix.max_blocks;
+    float* bscore_cta = a.bscore + static_cast<size_t>(blockIdx.x) * nwarps * maxb;
+    uint16_t* order = a.order + static_cast<size_t>(blockIdx.x) * a.order_stride;
+    unsigned long long* keys_g =
+        a.sortkeys != nullptr ? a.sortkeys + static_cast<size_t>(blockIdx.x) * a.sort_stride
+                              : nullptr;
+
+    for (int i = tid; i <= dim; i += blockDim.x) tbl[i] = 0;
+    if (tid == 0) qv[0] = 0.0f;
+
+    int iter = 0;
+    for (;;) {
+        if (tid == 0) {
+            int q;
+            if (a.work_counter != nullptr)
+                q = atomicAdd(a.work_counter, 1);
+            else
+                q = a.first_query + blockIdx.x + iter * gridDim.x;
+            ctl->q = q;
+        }
+        ++iter;
+        __syncthreads();
+        const int q = ctl->q;
+        if (q >= a.q.n) break;
+
+        // 1. scatter the query
+        const int32_t qs = a.q.indptr[q];
+        int qn = a.q.indptr[q + 1] - qs;
+        if (qn > a.qcap || qn < 0) {  // the caller's max_nnz was wrong: padding
+            if (tid == 0) atomicExch(a.err, 3);
+            qn = 0;
+        }
+        bool bad = false;
+        for (int i = tid; i < qn; i += blockDim.x) {
+            const uint32_t t = a.q.idx[qs + i];
+            const V v = static_cast<const V*>(a.q.val)[qs + i];
+            qterm[i] = static_cast<uint16_t>(t);
+            qraw[i] = v;
+            if (t < static_cast<uint32_t>(dim)) {
+                if constexpr (kRank) {
+                    tbl[t] = static_cast<TE>(i + 1);
+                } else {
+                    tbl[t] = static_cast<TE>(v);
+                }
+            }
+            if constexpr (kRank) {
+                qv[i + 1] = ValT<V>::f(v);
+                bad |= !isfinite(ValT<V>::f(v));
+            }
+        }
+        const bool nonfinite = __syncthreads_or(bad) != 0;
+
+        // 2. query cut: value desc, position asc; original order if cut >= nnz
+        int ncut;
+        if (a.cut >= qn) {
+            ncut = qn;
+            for (int i = tid; i < qn; i += blockDim.x) cuts[i] = qterm[i];
+        } else {
+            ncut = a.cut;
+            for (int i = tid; i < qn; i += blockDim.x) {
+                const float vi = ValT<V>::f(qraw[i]);
+                int rank = 0;
+                for (int j = 0; j < qn; ++j) {
+                    const float vj = ValT<V>::f(qraw[j]);
+                    rank += (vj > vi || (vj == vi && j < i)) ? 1 : 0;
+                }
+                if (rank < ncut) cuts[rank] = qterm[i];
+            }
+        }
+        __syncthreads();
+
+        int n = 0;  // heap size (warp 0)
+        bool first = true;
+        unsigned long long docs_scored = 0, blocks_visited = 0, bytes = 0, lists = 0,
+                           lane_bytes = 0;
+        for (int c = 0; c < ncut; ++c) {
+            // 3. summary scores of the next nwarps lists, one warp per list
+            if (c % nwarps == 0) {
+                const int cw = c + warp;
+                if (cw < ncut) {
+                    const int tw = cuts[cw];
+                    if (tw < a.ix.n_lists) {
+                        const int nbw = static_cast<int>(a.ix.lbp[tw + 1] - a.ix.lbp[tw]);
+                        if (nbw > 0)
+                            list_summaries<V>(a, tw, nbw, qterm, qraw, qn,
+                                              bscore_cta + static_cast<size_t>(warp) * maxb,
+                                              lane, bytes);
+                    }
+                }
+                __syncthreads();
+            }
+            const int t = cuts[c];
+            if (t >= a.ix.n_lists) continue;  // seismic_index.cpp:254-256
+            const int64_t lb0 = a.ix.lbp[t];
+            const int nb = static_cast<int>(a.ix.lbp[t + 1] - lb0);
+            if (nb > 0) {
+                ++lists;
+                const float* bscore = bscore_cta + static_cast<size_t>(c % nwarps) * maxb;
+                // 4. visiting order of the first list
+                if (first) {
+                    int p2 = 1;
+                    while (p2 < nb) p2 <<= 1;
+                    unsigned long long* keys = p2 <= 2 * batch
+                                                   ? reinterpret_cast<unsigned long long*>(cdoc)
+                                                   : keys_g;
+                    if (keys == nullptr) {  // the host sizes sortkeys; never taken
+                        if (tid == 0) atomicExch(a.err, 2);
+                        break;
+                    }
+                    sort_blocks(bscore, nb, keys, p2, order, tid, blockDim.x);
+                }
+                // 5. batches
+                Cursor cur;
+                cur.o = 0;
+                cur.dead = false;
+                cur.split = false;
+                cur.split_d = 0;
+                cur.split_left = 0;
+                cur.split_blk = 0;
+                cur.split_bs = 0.0f;
+                for (;;) {
+                    if (warp == 0) {
+                        int total = 0;
+                        const int nseg = gather(a, cur, first, lb0, nb, bscore, order, n, hs,
+                                                segs, batch, total, lane);
+                        if (lane == 0) {
+                            ctl->nseg = nseg;
+                            ctl->total = total;
+                            ctl->next = 0;
+                        }
+                    }
+                    __syncthreads();
+                    const int nseg = ctl->nseg;
+                    const int total = ctl->total;
+                    if (nseg == 0) break;
+                    if (total > 0) {
+                        // candidates: doc ids and row info of every segment's docs
+                        for (int i = tid; i < total; i += blockDim.x) {
+                            int lo = 0, hi = nseg - 1;
+                            while (lo < hi) {
+                                const int mid = (lo + hi + 1) >> 1;
+                                if (segs[mid].cand0 <= i)
+                                    lo = mid;
+                                else
+                                    hi = mid - 1;
+                            }
+                            const Seg& g = segs[lo];
+                            const int32_t d = __ldg(a.ix.docs + g.d0 + (i - g.cand0));
+                            bool member = true;
+                            if (a.sel_bits != nullptr)
+                                member = (__ldg(a.sel_bits + (d >> 6)) >> (d & 63)) & 1ull;
+                            uint2 ri = make_uint2(0u, 0u);
+                            if (member) ri = __ldg(a.fwd.rowinfo + d);
+                            cdoc[i] = member ? d : -1;
+                            coff[i] = ri.x;
+                            clen[i] = ri.y;
+                        }
+                        __syncthreads();
+                        // 6. scores
+                        if constexpr (kRank) {
+                            if (nonfinite)
+                                score_batch<V, TE, true, kG>(a.fwd, ctl, tbl, qv, coff, clen, csc,
+                                                             total, lane);
+                            else
+                                score_batch<V, TE, false, kG>(a.fwd, ctl, tbl, qv, coff, clen,
+                                                              csc, total, lane);
+                        } else {
+                            score_batch<V, TE, false, kG>(a.fwd, ctl, tbl, qv, coff, clen, csc,
+                                                          total, lane);
+                        }
+                        __syncthreads();
+                    }
+                    // 7. second pruning test and heap offers, in block order
+                    if (warp == 0) {
+                        for (int s = 0; s < nseg; ++s) {
+                            const Seg g = segs[s];
+                            if (g.head) {
+                                if (n == a.k && __fmul_rn(g.bs, a.heap_factor) < hs[a.k - 1]) {
+                                    if (first) {
+                                        cur.dead = true;
+                                        cur.split = false;
+                                        break;
+                                    }
+                                    if (s == nseg - 1) cur.split = false;
+                                    continue;
+                                }
+                                ++blocks_visited;
+                                bytes += 16;
+                            }
+                            bytes += 4ull * static_cast<unsigned long long>(g.cnt);
+                            for (int b = 0; b < g.cnt; b += 32) {
+                                const int j = b + lane;
+                                float sc = 0.0f;
+                                int32_t d = -1;
+                                if (j < g.cnt) {
+                                    d = cdoc[g.cand0 + j];
+                                    sc = csc[g.cand0 + j];
+                                }
+                                const bool mem = d >= 0;
+                                if (mem)
+                                    lane_bytes += 8ull + static_cast<unsigned long long>(
+                                                             clen[g.cand0 + j]) * (2 + vsz);
+                                docs_scored += __popc(__ballot_sync(kFull, mem));
+                                unsigned m =
+                                    __ballot_sync(kFull, mem && (n < a.k || sc > hs[a.k - 1]));
+                                while (m) {
+                                    const int src = __ffs(m) - 1;
+                                    m &= m - 1;
+                                    const float S = __shfl_sync(kFull, sc, src);
+                                    const int32_t D = __shfl_sync(kFull, d, src);
+                                    heap_offer(S, D, hs, hid, n, a.k, lane);
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            first = false;  // seismic_index.cpp:261
+        }
+
+        // results, padded with (-1.0, -1); SQ scores decoded
+        // (seismic_scalar_quantized_index.cpp:345-355)
+        if (warp == 0) {
+            float* od = a.out_d + static_cast<size_t>(q) * a.k;
+            int32_t* ol = a.out_l + static_cast<size_t>(q) * a.k;
+            for (int i = lane; i < a.k; i += 32) {
+                if (i < n) {
+                    const float s = hs[i];
+                    od[i] = a.decode_scale != 0.0f ? __fmul_rn(s, a.decode_scale) : s;
+                    ol[i] = hid[i];
+                } else {
+                    od[i] = -1.0f;
+                    ol[i] = -1;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) lane_bytes += __shfl_xor_sync(kFull, lane_bytes, o);
+        }
+        // lane 0 of every warp adds the warp's summary bytes
+        if (a.stats != nullptr && lane == 0) {
+            if (warp == 0) {
+                atomicAdd(a.stats + kStatDocsScored, docs_scored);
+                atomicAdd(a.stats + kStatBlocksVisited, blocks_visited);
+                atomicAdd(a.stats + kStatListsProbed, lists);
+                bytes += lane_bytes;
+            }
+            atomicAdd(a.stats + kStatBytes, bytes);
+        }
+        // restore the all-zero table for the next query
+        __syncthreads();
+        for (int i = tid; i < qn; i += blockDim.x) {
+            const uint32_t t = qterm[i];
+            if (t < static_cast<uint32_t>(dim)) tbl[t] = 0;
+        }
+    }
+}
+
+template <typename V, typename TE>
+size_t smem_typed(int dim, int qcap, int k, int batch) {
+    return cta_layout(static_cast<int>(sizeof(V)), static_cast<int>(sizeof(TE)), dim, qcap, k,
+                      batch)
+        .total;
+}
+
+template <typename V, typename TE, int kG>
+int max_blocks_cta_g(int threads, size_t smem) {
+    if (cudaFuncSetAttribute(seismic_cta_kernel<V, TE, kG>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem)) != cudaSuccess)
+        return 0;
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, seismic_cta_kernel<V, TE, kG>,
+                                                      threads, smem) != cudaSuccess)
+        return 0;
+    return blocks;
+}
+
+template <typename V, typename TE>
+int max_blocks_cta_typed(int group, int threads, size_t smem) {
+    if (group == 4) return max_blocks_cta_g<V, TE, 4>(threads, smem);
+    if (group == 2) return max_blocks_cta_g<V, TE, 2>(threads, smem);
+    return max_blocks_cta_g<V, TE, 1>(threads, smem);
+}
+
+template <typename V, typename TE, int kG>
+cudaError_t launch_cta_g(const SeismicLaunch& a, int warps, int blocks, size_t smem,
+                         cudaStream_t s) {
+    cudaError_t e = cudaFuncSetAttribute(seismic_cta_kernel<V, TE, kG>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    seismic_cta_kernel<V, TE, kG><<<blocks, warps * 32, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename V, typename TE>
+cudaError_t launch_cta_typed(const SeismicLaunch& a, int warps, int blocks, cudaStream_t s) {
+    const size_t smem = smem_typed<V, TE>(a.fwd.dim, a.qcap, a.k, a.batch_docs);
+    if (a.group_lanes == 4) return launch_cta_g<V, TE, 4>(a, warps, blocks, smem, s);
+    if (a.group_lanes == 2) return launch_cta_g<V, TE, 2>(a, warps, blocks, smem, s);
+    return launch_cta_g<V, TE, 1>(a, warps, blocks, smem, s);
+}
+
+}  // namespace
+
+// Table entries: fp32 queries hold ranks, one byte while the query has at
+// most 255 terms; SQ queries hold their codes.
+static bool wide_table(int val_kind, int qcap) {
+    return val_kind == kU16 || (val_kind == kF32 && qcap > 255);
+}
+
+size_t seismic_cta_smem(int val_kind, int dim, int qcap, int k, int batch) {
+    if (val_kind == kF32)
+        return wide_table(val_kind, qcap) ? smem_typed<float, uint16_t>(dim, qcap, k, batch)
+                                          : smem_typed<float, uint8_t>(dim, qcap, k, batch);
+    if (val_kind == kU8) return smem_typed<uint8_t, uint8_t>(dim, qcap, k, batch);
+    return smem_typed<uint16_t, uint16_t>(dim, qcap, k, batch);
+}
+
+int seismic_cta_max_blocks_per_sm(int val_kind, int qcap, int group, int warps, size_t smem) {
+    const int th = warps * 32;
+    if (val_kind == kF32)
+        return wide_table(val_kind, qcap)
+                   ? max_blocks_cta_typed<float, uint16_t>(group, th, smem)
+                   : max_blocks_cta_typed<float, uint8_t>(group, th, smem);
+    if (val_kind == kU8) return max_blocks_cta_typed<uint8_t, uint8_t>(group, th, smem);
+    return max_blocks_cta_typed<uint16_t, uint16_t>(group, th, smem);
+}
+
+cudaError_t launch_seismic_cta(int val_kind, const SeismicLaunch& a, int warps, int blocks,
+                               cudaStream_t s) {
+    if (val_kind == kF32)
+        return wide_table(val_kind, a.qcap) ? launch_cta_typed<float, uint16_t>(a, warps, blocks, s)
+                                            : launch_cta_typed<float, uint8_t>(a, warps, blocks, s);
+    if (val_kind == kU8) return launch_cta_typed<uint8_t, uint8_t>(a, warps, blocks, s);
+    return launch_cta_typed<uint16_t, uint16_t>(a, warps, blocks, s);
+}
+
+}  // namespace nsp

@@ -163,7 +163,8 @@ def test_seismic_plain_equals_batched(seismic_file):
         np.testing.assert_array_equal(Dw, Db)
 
 
-@pytest.mark.parametrize("variant,stage", [(0, 0), (1, 0), (1, 2048), (1, 128)])
+@pytest.mark.parametrize("variant,stage", [(0, 0), (1, 0), (1, 2048), (1, 128), (2, 0), (2, 32),
+                                           (3, 0), (4, 64)])
 @pytest.mark.parametrize("kind", ["fp32", "sq8"])
 def test_seismic_kernel_variants_agree(tmp_path, variant, stage, kind):
     """Direct row loads, bulk-copy staging, and staging buffers so small that
@@ -192,6 +193,56 @@ def test_seismic_kernel_variants_agree(tmp_path, variant, stage, kind):
     b2.set_kernel(0, 0)
     b2.set_id_selector(sel)
     np.testing.assert_array_equal(search(idx, qs, params=p2)[1], search(idx, qs, params=b2)[1])
+
+
+@pytest.mark.parametrize("kind", ["fp32", "sq8"])
+def test_cta_kernel_batches_split_blocks_and_sorts_in_hbm(tmp_path, kind):
+    """One CTA per query: blocks of hundreds of docs split across batches of
+    32, the first list (up to 200 blocks) sorted in global scratch, selector
+    filtering, 1, 2 and 4 lanes per doc -- results equal the oracle's bit for
+    bit at every batch size."""
+    docs = synth.docs_config0(20000, seed=5)
+    qs = synth.queries_config0(200, seed=6)
+    vmin, vmax = float(docs.values.min()), float(docs.values.max())
+    spec = ("seismic,lambda=2000|beta=200|alpha=0.4|seed=7" if kind == "fp32"
+            else sq_spec(vmin, vmax, lam=2000, beta=200))
+    idx = make(spec, docs)
+    nsparse.write_index(idx, str(tmp_path / "c.idx"))
+    codes = None if kind == "fp32" else O.sq_encode_u8(vmin, vmax, qs.values)
+    ids = np.arange(0, docs.n, 2, dtype=np.int32)
+    Do, Lo = oracle_seismic_from_file(tmp_path / "c.idx", qs, K, CUT, HF, codes=codes)
+    Dos, Los = oracle_seismic_from_file(tmp_path / "c.idx", qs, K, CUT, HF, codes=codes,
+                                        sel_bits=O.bitmap_from_ids(docs.n, ids))
+    if kind != "fp32":
+        scale = np.float32(O.sq_scale(vmin, vmax, vmin, vmax))
+        Do = np.where(Lo >= 0, (Do * scale).astype(np.float32), Do)
+        Dos = np.where(Los >= 0, (Dos * scale).astype(np.float32), Dos)
+    for variant, batch in ((2, 0), (2, 32), (2, 96), (2, 4096), (3, 64), (4, 0), (4, 32)):
+        p = nsparse.SeismicSearchParameters(CUT, HF)
+        p.set_kernel(variant, batch)
+        D, L = search(idx, qs, params=p)
+        np.testing.assert_array_equal(L, Lo)
+        np.testing.assert_array_equal(D, Do)
+        p.set_id_selector(nsparse.SetIDSelector(ids))
+        Ds, Ls = search(idx, qs, params=p)
+        np.testing.assert_array_equal(Ls, Los)
+        np.testing.assert_array_equal(Ds, Dos)
+
+
+def test_cta_kernel_non_finite_query_value(seismic_file):
+    """A query value of +inf: row padding must not turn sums into NaN."""
+    _, qs = golden_corpus()
+    vals = qs.values.copy()
+    vals[qs.indptr[3]] = np.inf
+    qi = synth.Csr(qs.dim, qs.indptr, qs.indices, vals)
+    Do, Lo = oracle_seismic_from_file(seismic_file, qi, K, CUT, HF)
+    idx = nsparse.read_index(str(seismic_file))
+    for variant in (2, 3, 4):
+        p = nsparse.SeismicSearchParameters(CUT, HF)
+        p.set_kernel(variant, 0)
+        D, L = search(idx, qi, params=p)
+        np.testing.assert_array_equal(L, Lo)
+        np.testing.assert_array_equal(D, Do)
 
 
 def test_seismic_filter_and_exact_path_match_golden(seismic_file):
