@@ -22,8 +22,8 @@ struct EngineOptions {
     int warps_per_block = 0;
     // SEISMIC kernel variant: -1 lets the engine choose, 0 one warp per query
     // loading doc rows straight from HBM, 1 the same with rows staged in
-    // shared memory by bulk copy (stage_bytes per buffer, 0 = default), 2-4
-    // one CTA per query with 1, 2 or 4 lanes per scored doc, in batches of
+    // shared memory by bulk copy (stage_bytes per buffer, 0 = default), 2-5
+    // one CTA per query with 1, 2, 4 or 8 lanes per scored doc, in batches of
     // batch_docs candidate docs (0 = default). Results are identical.
     int variant = -1;
     int stage_bytes = 0;

@@ -122,8 +122,8 @@ nsp_status_t nsp_search_params_set_engine(nsp_search_params_t* params, int plain
                                           int warps_per_block);
 /* Extension: SEISMIC kernel variant (-1 engine's choice, 0 one warp per query
  * with direct row loads, 1 the same with rows staged in shared memory by bulk
- * copy, 2-4 one CTA per query with 1, 2 or 4 lanes per scored doc) and its
- * tuning value: variant 1's buffer size in bytes, variants 2-4's candidate
+ * copy, 2-5 one CTA per query with 1, 2, 4 or 8 lanes per scored doc) and its
+ * tuning value: variant 1's buffer size in bytes, variants 2-5's candidate
  * docs per batch (0 = default). Results do not depend on either. */
 nsp_status_t nsp_search_params_set_kernel(nsp_search_params_t* params, int variant,
                                           int tuning);

@@ -241,7 +241,7 @@ nsp_status_t nsp_search_params_set_kernel(nsp_search_params_t* params, int varia
                                           int tuning) {
     return guarded([&] {
         if (params == nullptr) throw std::invalid_argument("unexpected nullptr");
-        if (variant < -1 || variant > 4) throw std::invalid_argument("variant must be in [-1, 4]");
+        if (variant < -1 || variant > 5) throw std::invalid_argument("variant must be in [-1, 5]");
         auto& e = as_params(params)->engine;
         e.variant = variant;
         e.stage_bytes = 0;

@@ -447,12 +447,12 @@ struct SeismicPlan {
     int variant;
     int stage_bytes;
     int bcap;
-    int batch_docs;   // variants 2-4
-    size_t smem_cta;  // variants 2-4
-    int group_lanes;  // variants 2-4: lanes per scored doc
+    int batch_docs;   // variants 2-5
+    size_t smem_cta;  // variants 2-5
+    int group_lanes;  // variants 2-5: lanes per scored doc
 };
 
-// Variants 2-4 (one CTA per query): 8 warps and batches of 512 candidate docs
+// Variants 2-5 (one CTA per query): 8 warps and batches of 512 candidate docs
 // unless asked otherwise; the batch shrinks if shared memory is short.
 SeismicPlan plan_seismic_cta(int kind, int dim, int qcap, int k, int n_queries,
                              const SeismicSearchArgs& args, bool single) {
@@ -469,7 +469,7 @@ SeismicPlan plan_seismic_cta(int kind, int dim, int qcap, int k, int n_queries,
         throw std::invalid_argument("query too long or k too large for the device search kernel");
     p.batch_docs = batch;
     p.wpb = warps;
-    p.group_lanes = args.variant == 4 ? 4 : (args.variant == 3 ? 2 : 1);
+    p.group_lanes = 1 << std::min(std::max(args.variant - 2, 0), 3);  // 2..5 -> 1..8
     int per_sm = seismic_cta_max_blocks_per_sm(kind, qcap, p.group_lanes, warps, p.smem_cta);
     if (per_sm < 1) per_sm = 1;
     p.blocks = single ? 1 : std::max(1, std::min(n_queries, device_sm_count() * per_sm));

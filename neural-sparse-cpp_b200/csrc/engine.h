@@ -206,9 +206,9 @@ struct SeismicSearchArgs {
     bool plain = false;       // one query per launch
     int warps_per_block = 0;  // 0 = autotuned
     int variant = -1;         // -1 auto, 0 direct row loads, 1 bulk-copy staged rows,
-                              // 2-4 one CTA per query with 1, 2, 4 lanes per doc
+                              // 2-5 one CTA per query with 1, 2, 4, 8 lanes per doc
     int stage_bytes = 0;      // staged: bytes per stage buffer (0 = default)
-    int batch_docs = 0;       // variants 2-4: candidate docs per batch (0 = default)
+    int batch_docs = 0;       // variants 2-5: candidate docs per batch (0 = default)
 };
 
 // Host buffers in, host buffers out (the reference-facing path).

@@ -98,8 +98,8 @@ struct SeismicLaunch {
     int32_t stage_bytes;
     int32_t bcap;
     int32_t* err;               // nonzero: a kernel-side error (see check_kernel_error)
-    // Variants 2-4 (one CTA per query): candidate docs per batch, lanes per
-    // scored doc (1, 2, 4), and per-CTA scratch -- `bscore` holds warps *
+    // Variants 2-5 (one CTA per query): candidate docs per batch, lanes per
+    // scored doc (1, 2, 4, 8), and per-CTA scratch -- `bscore` holds warps *
     // max_blocks floats per CTA, `order` the first list's visiting order,
     // `sortkeys` the sort buffer of lists too long to sort in shared memory
     // (nullptr when none is).
@@ -138,7 +138,7 @@ cudaError_t launch_seismic(int val_kind, const SeismicLaunch& a, int warps_per_b
 int seismic_max_blocks_per_sm(int val_kind, int variant, int warps_per_block, size_t smem);
 int seismic_max_blocks_per_sm(int val_kind, int warps_per_block, size_t smem);  // variant 0
 
-// Variants 2-4: one CTA of `warps` warps per query (search_seismic_cta.cu).
+// Variants 2-5: one CTA of `warps` warps per query (search_seismic_cta.cu).
 size_t seismic_cta_smem(int val_kind, int dim, int qcap, int k, int batch_docs);
 int seismic_cta_max_blocks_per_sm(int val_kind, int qcap, int group_lanes, int warps,
                                   size_t smem);

@@ -1,5 +1,5 @@
 // SEISMIC / SEISMIC-SQ search on sm_100a, one CTA per query (kernel
-// variants 2-4). A persistent grid steals queries from a global counter; the
+// variants 2-5). A persistent grid steals queries from a global counter; the
 // CTA's warps walk the query's blocks together.
 //
 // Per query (seismic_index.cpp:231-274, seismic_scalar_quantized_index.cpp:
@@ -25,7 +25,7 @@
 //      reference tests it, and its docs are offered in order. Docs of a block
 //      that fails the second test are dropped: the result is the reference's,
 //      only some scoring work is speculative;
-//   6. a group of kG lanes (1, 2 or 4) scores one doc at a time, 16 row
+//   6. a group of kG lanes (1, 2, 4 or 8) scores one doc at a time, 16 row
 //      elements per lane per step from 256-bit loads of the padded forward
 //      rows, and takes the next doc of the batch as soon as its row ends, so
 //      groups stay busy across rows of different lengths. fp32 scores are the
@@ -815,6 +815,7 @@ int max_blocks_cta_g(int threads, size_t smem) {
 
 template <typename V, typename TE>
 int max_blocks_cta_typed(int group, int threads, size_t smem) {
+    if (group == 8) return max_blocks_cta_g<V, TE, 8>(threads, smem);
     if (group == 4) return max_blocks_cta_g<V, TE, 4>(threads, smem);
     if (group == 2) return max_blocks_cta_g<V, TE, 2>(threads, smem);
     return max_blocks_cta_g<V, TE, 1>(threads, smem);
@@ -834,6 +835,7 @@ cudaError_t launch_cta_g(const SeismicLaunch& a, int warps, int blocks, size_t s
 template <typename V, typename TE>
 cudaError_t launch_cta_typed(const SeismicLaunch& a, int warps, int blocks, cudaStream_t s) {
     const size_t smem = smem_typed<V, TE>(a.fwd.dim, a.qcap, a.k, a.batch_docs);
+    if (a.group_lanes == 8) return launch_cta_g<V, TE, 8>(a, warps, blocks, smem, s);
     if (a.group_lanes == 4) return launch_cta_g<V, TE, 4>(a, warps, blocks, smem, s);
     if (a.group_lanes == 2) return launch_cta_g<V, TE, 2>(a, warps, blocks, smem, s);
     return launch_cta_g<V, TE, 1>(a, warps, blocks, smem, s);

@@ -188,9 +188,9 @@ class SearchParameters:
 
     def set_kernel(self, variant=-1, tuning=0):
         """Extension: SEISMIC kernel variant (-1 auto, 0 warp per query with
-        direct loads, 1 warp per query with bulk-copy staging, 2-4 CTA per
-        query with 1, 2 or 4 lanes per doc) and its tuning value (variant 1:
-        staging buffer bytes; variants 2-4: candidate docs per batch; 0 =
+        direct loads, 1 warp per query with bulk-copy staging, 2-5 CTA per
+        query with 1, 2, 4 or 8 lanes per doc) and its tuning value (variant 1:
+        staging buffer bytes; variants 2-5: candidate docs per batch; 0 =
         default). Results do not depend on either."""
         _check(_L.nsp_search_params_set_kernel(self._h, int(variant), int(tuning)))
 

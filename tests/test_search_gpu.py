@@ -164,7 +164,7 @@ def test_seismic_plain_equals_batched(seismic_file):
 
 
 @pytest.mark.parametrize("variant,stage", [(0, 0), (1, 0), (1, 2048), (1, 128), (2, 0), (2, 32),
-                                           (3, 0), (4, 64)])
+                                           (3, 0), (4, 64), (5, 0)])
 @pytest.mark.parametrize("kind", ["fp32", "sq8"])
 def test_seismic_kernel_variants_agree(tmp_path, variant, stage, kind):
     """Direct row loads, bulk-copy staging, and staging buffers so small that
@@ -199,7 +199,7 @@ def test_seismic_kernel_variants_agree(tmp_path, variant, stage, kind):
 def test_cta_kernel_batches_split_blocks_and_sorts_in_hbm(tmp_path, kind):
     """One CTA per query: blocks of hundreds of docs split across batches of
     32, the first list (up to 200 blocks) sorted in global scratch, selector
-    filtering, 1, 2 and 4 lanes per doc -- results equal the oracle's bit for
+    filtering, 1, 2, 4 and 8 lanes per doc -- results equal the oracle's bit for
     bit at every batch size."""
     docs = synth.docs_config0(20000, seed=5)
     qs = synth.queries_config0(200, seed=6)
@@ -217,7 +217,8 @@ def test_cta_kernel_batches_split_blocks_and_sorts_in_hbm(tmp_path, kind):
         scale = np.float32(O.sq_scale(vmin, vmax, vmin, vmax))
         Do = np.where(Lo >= 0, (Do * scale).astype(np.float32), Do)
         Dos = np.where(Los >= 0, (Dos * scale).astype(np.float32), Dos)
-    for variant, batch in ((2, 0), (2, 32), (2, 96), (2, 4096), (3, 64), (4, 0), (4, 32)):
+    for variant, batch in ((2, 0), (2, 32), (2, 96), (2, 4096), (3, 64), (4, 0), (4, 32), (5, 0),
+                           (5, 64)):
         p = nsparse.SeismicSearchParameters(CUT, HF)
         p.set_kernel(variant, batch)
         D, L = search(idx, qs, params=p)
@@ -237,7 +238,7 @@ def test_cta_kernel_non_finite_query_value(seismic_file):
     qi = synth.Csr(qs.dim, qs.indptr, qs.indices, vals)
     Do, Lo = oracle_seismic_from_file(seismic_file, qi, K, CUT, HF)
     idx = nsparse.read_index(str(seismic_file))
-    for variant in (2, 3, 4):
+    for variant in (2, 3, 4, 5):
         p = nsparse.SeismicSearchParameters(CUT, HF)
         p.set_kernel(variant, 0)
         D, L = search(idx, qi, params=p)
