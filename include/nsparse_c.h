@@ -184,6 +184,18 @@ nsp_status_t nsp_index_search_device_noalloc(nsp_index_t* index, int32_t n,
                                              int32_t* d_labels, const nsp_search_params_t* params,
                                              void* cuda_stream);
 
+/* Kernel autotuner. Times each one-CTA-per-query launch shape of the SEISMIC
+ * search (lanes per doc, candidate docs per batch, warps per CTA) on the n
+ * sample queries with the given parameters and keeps the fastest for this
+ * index: later searches whose parameters leave the kernel to the engine
+ * (variant -1) use it. Results do not depend on the choice. Writes the choice
+ * to the out pointers (any may be NULL). Extension with no counterpart in the
+ * reference. */
+nsp_status_t nsp_index_autotune(nsp_index_t* index, int32_t n, const int32_t* indptr,
+                                const uint16_t* indices, const float* values, int k,
+                                const nsp_search_params_t* params, int* variant, int* batch_docs,
+                                int* warps_per_block, float* kernel_ms);
+
 /* Number of CUDA devices visible and the name of the current one. */
 nsp_status_t nsp_device_info(int32_t* n_devices, char* name, size_t name_len);
 

@@ -287,6 +287,21 @@ nsp_status_t nsp_index_search_device(nsp_index_t* index, int32_t n, const int32_
     });
 }
 
+nsp_status_t nsp_index_autotune(nsp_index_t* index, int32_t n, const int32_t* indptr,
+                                const uint16_t* indices, const float* values, int k,
+                                const nsp_search_params_t* params, int* variant, int* batch_docs,
+                                int* warps_per_block, float* kernel_ms) {
+    return guarded([&] {
+        if (index == nullptr) throw std::invalid_argument("unexpected nullptr");
+        const nsp::KernelChoice c = detail::seismic_autotune(
+            as_index(index), n, indptr, indices, values, k, as_params(params));
+        if (variant != nullptr) *variant = c.variant;
+        if (batch_docs != nullptr) *batch_docs = c.batch_docs;
+        if (warps_per_block != nullptr) *warps_per_block = c.warps_per_block;
+        if (kernel_ms != nullptr) *kernel_ms = c.kernel_ms;
+    });
+}
+
 nsp_status_t nsp_device_info(int32_t* n_devices, char* name, size_t name_len) {
     return guarded([&] {
         int n = 0;

@@ -195,6 +195,14 @@ struct SearchStats {
     int launches = 0;
 };
 
+// A SEISMIC kernel launch shape chosen by the autotuner (variant < 0: none).
+struct KernelChoice {
+    int variant = -1;
+    int batch_docs = 0;
+    int warps_per_block = 0;
+    float kernel_ms = 0.0f;  // on the tuning sample
+};
+
 struct SeismicSearchArgs {
     int k = 10;
     int cut = 10;

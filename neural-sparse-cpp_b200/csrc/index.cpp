@@ -348,10 +348,19 @@ const IDSelectorEnumerable* exact_match_selector(const IDSelector* sel, int k) {
     return en->size() <= static_cast<size_t>(k) ? en : nullptr;
 }
 
+// The autotuner's launch shape, where the caller left the choice to the engine.
+void apply_tuned(const SeismicState& st, nsp::SeismicSearchArgs& a) {
+    if (a.variant >= 0 || st.tuned.variant < 0) return;
+    a.variant = st.tuned.variant;
+    if (a.batch_docs == 0) a.batch_docs = st.tuned.batch_docs;
+    if (a.warps_per_block == 0) a.warps_per_block = st.tuned.warps_per_block;
+}
+
 void seismic_search_common(SeismicState& st, int dim, idx_t n, const idx_t* indptr,
                            const term_t* indices, const float* values, int k, float* distances,
                            idx_t* labels, SearchParameters* params, nsp::SeismicSearchArgs args) {
     if (st.vectors.host.n() == 0) return fill_padding(n, k, distances, labels);
+    apply_tuned(st, args);
     st.vectors.ensure_device();
     const nsp::QueryBatch q = nsp::canonicalize(n, indptr, indices, values, dim);
     const IDSelector* sel = params == nullptr ? nullptr : params->get_id_selector();
@@ -544,6 +553,7 @@ void search_device(Index* index, int32_t n, const int32_t* d_indptr, const uint1
     }
     if (st->vectors.host.n() == 0) throw std::runtime_error("index is empty");
     if (max_nnz < 0) throw std::invalid_argument("max_row_nnz must not be negative");
+    apply_tuned(*st, a);
     const IDSelector* sel = params == nullptr ? nullptr : params->get_id_selector();
     if (exact_match_selector(sel, k) != nullptr)
         throw std::invalid_argument("device-resident search does not take the exact-match path");
@@ -573,6 +583,66 @@ void search_device(Index* index, int32_t n, const int32_t* d_indptr, const uint1
     }
     nsp::seismic_search_device(st->vectors.dev, st->lists_dev, n, d_indptr, d_idx, vals, max_nnz,
                                a, d_sel, d_out, d_lab, s, nullptr);
+}
+
+nsp::KernelChoice seismic_autotune(Index* index, idx_t n, const idx_t* indptr,
+                                   const term_t* indices, const float* values, int k,
+                                   SearchParameters* params) {
+    throw_if_not_positive(n);
+    throw_if_not_positive(k);
+    throw_if_any_null(indptr, indices, values);
+    if (auto* im = dynamic_cast<IDMapIndex*>(index)) index = im->delegate();
+    SeismicState* st = nullptr;
+    nsp::SeismicSearchArgs a = seismic_args(params, k);
+    if (auto* si = dynamic_cast<SeismicIndex*>(index)) {
+        st = si->state();
+    } else if (auto* qi = dynamic_cast<SeismicScalarQuantizedIndex*>(index)) {
+        st = qi->state();
+        const auto* sqp = dynamic_cast<const SeismicSQSearchParameters*>(params);
+        const ScalarQuantizer& isq = qi->get_scalar_quantizer();
+        const ScalarQuantizer qsq =
+            sqp == nullptr ? isq : ScalarQuantizer(isq.get_quantizer_type(), sqp->vmin, sqp->vmax);
+        a.qbits = isq.bits();
+        a.q_vmin = qsq.get_min();
+        a.q_scale = qsq.encode_scale();
+        a.decode_scale = isq.decode_scale(qsq);
+    } else {
+        throw std::invalid_argument("autotune applies to seismic indexes");
+    }
+    if (st->vectors.host.n() == 0) throw std::runtime_error("index is empty");
+    st->vectors.ensure_device();
+    st->ensure_lists();
+    const nsp::QueryBatch q = nsp::canonicalize(n, indptr, indices, values, index->get_dimension());
+    std::vector<float> d(static_cast<size_t>(n) * k);
+    std::vector<idx_t> l(static_cast<size_t>(n) * k);
+    nsp::KernelChoice best;
+    for (int variant = 2; variant <= 5; ++variant) {
+        for (int batch : {256, 512, 1024}) {
+            for (int warps : {4, 8}) {
+                nsp::SeismicSearchArgs t = a;
+                t.variant = variant;
+                t.batch_docs = batch;
+                t.warps_per_block = warps;
+                t.plain = false;
+                float ms = 0.0f;
+                for (int rep = 0; rep < 2; ++rep) {  // the first run warms caches
+                    nsp::SearchStats s;
+                    nsp::seismic_search(st->vectors.dev, st->lists_dev, q, t, nullptr, d.data(),
+                                        l.data(), &s);
+                    ms = s.kernel_ms;
+                }
+                if (best.variant < 0 || ms < best.kernel_ms) {
+                    best.variant = variant;
+                    best.batch_docs = batch;
+                    best.warps_per_block = warps;
+                    best.kernel_ms = ms;
+                }
+            }
+        }
+    }
+    std::lock_guard<std::mutex> g(st->mu);
+    st->tuned = best;
+    return best;
 }
 
 }  // namespace detail

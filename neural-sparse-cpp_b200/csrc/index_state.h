@@ -38,6 +38,7 @@ struct SeismicState {
     nsp::SeismicDevice lists_dev;
     bool host_valid = false;
     bool dev_valid = false;
+    nsp::KernelChoice tuned;         // set by autotune; used when the caller leaves the choice
     std::mutex mu;
     // Uploads the host lists if the device copy is stale.
     void ensure_lists();
@@ -49,6 +50,13 @@ struct SeismicState {
 void seismic_build(SeismicState& st, int dim, const SeismicClusterParameters& params);
 
 std::vector<uint64_t> selector_bitmap(const IDSelector* sel, int64_t n_docs);
+
+// Times every one-CTA-per-query launch shape (lanes per doc x batch x warps)
+// on a sample of queries and keeps the fastest for later searches that leave
+// the kernel to the engine (seismic indexes, also through an IDMapIndex).
+nsp::KernelChoice seismic_autotune(Index* index, idx_t n, const idx_t* indptr,
+                                   const term_t* indices, const float* values, int k,
+                                   SearchParameters* params);
 
 // SEISMIC search over device-resident queries and results (nsparse_c.h,
 // nsp_index_search_device). Enqueues on `s` and returns.

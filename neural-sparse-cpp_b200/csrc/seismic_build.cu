@@ -518,6 +518,15 @@ __global__ void run_compact_kernel(const int64_t* flag, const int64_t* pos, int6
         if (flag[i]) run_start[pos[i]] = static_cast<int32_t>(i);
 }
 
+// The run index at each block's first entry (n_runs for a block past the
+// last entry); empty blocks are fixed up on the host.
+__global__ void block_first_run_kernel(const int64_t* pos, const int32_t* boff, int64_t nb,
+                                       int64_t ne, int64_t n_runs, int64_t* first_run) {
+    for (int64_t b = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; b < nb;
+         b += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        first_run[b] = boff[b] < ne ? pos[boff[b]] : n_runs;
+}
+
 __global__ void mass_kernel(const float* delta, const uint8_t* has_delta, const int32_t* boff,
                             int64_t nb, float* mass) {
     for (int64_t b = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; b < nb;
@@ -592,8 +601,12 @@ void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
     // pairs per block: the run index at each block's first entry
     std::vector<int64_t> pair_off(static_cast<size_t>(nb) + 1);
     {
-        const std::vector<int64_t> h_pos = to_host(pos, static_cast<size_t>(ne), s);
-        for (int64_t b = 0; b < nb; ++b) pair_off[b] = boff64[b] < ne ? h_pos[boff64[b]] : n_runs;
+        DevArray<int64_t> first_run(nb);
+        block_first_run_kernel<<<sms * 4, 256, 0, s>>>(pos.data(), d_boff.data(), nb, ne, n_runs,
+                                                       first_run.data());
+        cuda_check(cudaGetLastError(), "block_first_run_kernel");
+        const std::vector<int64_t> h_first = to_host(first_run, static_cast<size_t>(nb), s);
+        for (int64_t b = 0; b < nb; ++b) pair_off[b] = h_first[b];
         pair_off[nb] = n_runs;
         // an empty block has no runs: its offset is the next block's
         for (int64_t b = nb - 1; b >= 0; --b)

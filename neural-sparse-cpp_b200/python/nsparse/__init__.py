@@ -74,6 +74,8 @@ _sig("nsp_search_params_set_kernel", _P, ctypes.c_int, ctypes.c_int)
 _sig("nsp_search_params_free", _P)
 _sig("nsp_index_search_device", _P, _I32, _P, _P, _P, _I32, ctypes.c_int, _P, _P, _P, _P)
 _sig("nsp_device_info", ctypes.POINTER(_I32), ctypes.c_char_p, ctypes.c_size_t)
+_sig("nsp_index_autotune", _P, _I32, _P, _P, _P, ctypes.c_int, _P, ctypes.POINTER(ctypes.c_int),
+     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float))
 
 
 class _Stats(ctypes.Structure):
@@ -274,6 +276,22 @@ class Index:
         _check(_L.nsp_index_search_device(self._h, int(n), d_indptr, d_indices, d_values,
                                           int(max_row_nnz), int(k), d_distances, d_labels,
                                           None if params is None else params._h, stream))
+
+    def autotune(self, n, indptr, indices, values, k, params=None):
+        """Extension: times the SEISMIC kernel's launch shapes on these sample
+        queries and keeps the fastest for later searches that leave the kernel
+        to the engine. Returns the choice as a dict."""
+        indptr = np.ascontiguousarray(indptr, dtype=np.int32)
+        indices = np.ascontiguousarray(indices, dtype=np.uint16)
+        values = np.ascontiguousarray(values, dtype=np.float32)
+        v, b, w = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        ms = ctypes.c_float()
+        _check(_L.nsp_index_autotune(self._h, int(n), _ptr(indptr), _ptr(indices), _ptr(values),
+                                     int(k), None if params is None else params._h,
+                                     ctypes.byref(v), ctypes.byref(b), ctypes.byref(w),
+                                     ctypes.byref(ms)))
+        return {"variant": v.value, "batch_docs": b.value, "warps_per_block": w.value,
+                "kernel_ms": ms.value}
 
     def num_vectors(self):
         out = ctypes.c_int64()

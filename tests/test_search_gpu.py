@@ -246,6 +246,21 @@ def test_cta_kernel_non_finite_query_value(seismic_file):
         np.testing.assert_array_equal(D, Do)
 
 
+def test_autotune_picks_a_shape_and_keeps_results(seismic_file):
+    """The autotuner's choice is one of the CTA-per-query shapes and the
+    searches that follow it return the same ids and scores."""
+    _, qs = golden_corpus()
+    idx = nsparse.read_index(str(seismic_file))
+    p = nsparse.SeismicSearchParameters(CUT, HF)
+    D0, L0 = search(idx, qs, params=p)
+    c = idx.autotune(qs.n, qs.indptr, qs.indices, qs.values, K, p)
+    assert 2 <= c["variant"] <= 5 and c["batch_docs"] in (256, 512, 1024)
+    assert c["warps_per_block"] in (4, 8) and c["kernel_ms"] > 0
+    D1, L1 = search(idx, qs, params=p)
+    np.testing.assert_array_equal(L1, L0)
+    np.testing.assert_array_equal(D1, D0)
+
+
 def test_seismic_filter_and_exact_path_match_golden(seismic_file):
     g = golden()
     _, qs = golden_corpus()
