@@ -372,12 +372,12 @@ def run_engine(args):
 
 
 # SEISMIC-SQ at 8.8M docs: uint8 codes, uneven queries (nnz 5-200), posting
-# cap 6,000, 600 blocks per full list, cut 12, heap factor swept.
+# cap 6,000, 600 blocks per full list; (query cut, heap factor) swept: the
+# workload's cut 12 with heap factors 0.7-0.95, then wider cuts.
 SQ_DOCS = 8_800_000
 SQ_QUERIES = 65_536
 SQ_BATCH = 16_384
-SQ_CUT = 12
-SQ_HFS = (0.7, 0.8, 0.9, 0.95)
+SQ_SWEEP = ((12, 0.7), (12, 0.8), (12, 0.9), (12, 0.95), (20, 0.9), (30, 0.9), (40, 0.9))
 SQ_GT_QUERIES = 1000
 SQ_PLAIN = 200
 
@@ -401,6 +401,22 @@ def run_engine_sq(args):
     vmin, vmax = float(docs.values.min()), float(docs.values.max())
     spec = (f"seismic_sq,quantizer=8bit|vmin={vmin!r}|vmax={vmax!r}|lambda=6000|beta=600|"
             f"alpha=0.4|seed=7")
+    if args.kernel_only:
+        # build, then the batched search launches only (the profiling case)
+        idx = nsparse.index_factory(docs.dim, spec)
+        idx.add(docs.n, docs.indptr, docs.indices, docs.values)
+        idx.build()
+        params = nsparse.SeismicSearchParameters(12, 0.9)
+        params.set_kernel(args.variant, args.tuning)
+        q = qs.rows(0, SQ_BATCH)
+        for _ in range(max(args.warmup, 1) + args.steps):
+            idx.search(q.n, q.indptr, q.indices, q.values, K, params)
+        st = nsparse.last_search_stats()
+        print(json.dumps({"case": f"seismic_sq8_{docs.n}_docs_{q.n}_queries", "cut": 12,
+                          "heap_factor": 0.9, "kernel_ms": st.kernel_ms,
+                          "algorithmic_bytes": st.bytes,
+                          "docs_scored_per_query": st.docs_scored / q.n}))
+        return
     # exact fp32 ground truth first (its index is freed before the SQ build)
     t = time.perf_counter()
     exact = nsparse.index_factory(docs.dim, "inverted")
@@ -428,8 +444,8 @@ def run_engine_sq(args):
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     peak, peak_kind = measured_peaks()
     sweep = []
-    for hf in SQ_HFS:
-        params = nsparse.SeismicSearchParameters(SQ_CUT, hf)
+    for cut, hf in SQ_SWEEP:
+        params = nsparse.SeismicSearchParameters(cut, hf)
         params.set_kernel(args.variant, args.tuning)
 
         def one_pass():
@@ -462,7 +478,7 @@ def run_engine_sq(args):
         D1, L1 = idx.search(q1.n, q1.indptr, q1.indices, q1.values, K, params)
         st = nsparse.last_search_stats()
         assert (L1 == hL[:SQ_BATCH]).all() and (D1 == hD[:SQ_BATCH]).all()
-        plain = nsparse.SeismicSearchParameters(SQ_CUT, hf)
+        plain = nsparse.SeismicSearchParameters(cut, hf)
         plain.set_kernel(args.variant, args.tuning)
         plain.set_engine(plain=True)
         qp = qs.rows(0, SQ_PLAIN)
@@ -477,7 +493,7 @@ def run_engine_sq(args):
         lat_ms = sorted(1000 * x for x in lat)
         qps = qs.n / (ms / 1000.0)
         achieved = st.bytes / (st.kernel_ms / 1000.0) / 1e9
-        sweep.append({"heap_factor": hf, "qps": qps, "ms_per_pass": ms,
+        sweep.append({"cut": cut, "heap_factor": hf, "qps": qps, "ms_per_pass": ms,
                       "recall_at_10": recall_at_k(hL[:SQ_GT_QUERIES], Lt),
                       "plain_qps": SQ_PLAIN / sum(lat), "plain_p50_ms": lat_ms[len(lat_ms) // 2],
                       "plain_p99_ms": lat_ms[int(0.99 * (len(lat_ms) - 1))],
@@ -486,7 +502,8 @@ def run_engine_sq(args):
                       "docs_scored_per_query": st.docs_scored / q1.n})
         log(json.dumps(sweep[-1]))
     ok = [s for s in sweep if s["recall_at_10"] >= 0.95]
-    head = max(ok, key=lambda s: s["qps"]) if ok else sweep[-1]
+    head = max(ok, key=lambda s: s["qps"]) if ok else max(sweep, key=lambda s: s["recall_at_10"])
+    serving = serve_sweep(nsparse, idx, docs, qs, head["cut"], head["heap_factor"], args.serve_rates)
     out = {"metric": "QPS@recall@10>=0.95 (SEISMIC-SQ uint8, batched, 8.8M docs)",
            "value": head["qps"], "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
            "warmup": max(args.warmup, 1), "ms_per_step": head["ms_per_pass"],
@@ -495,11 +512,101 @@ def run_engine_sq(args):
            "config": {"workload": f"seismic_sq8_{docs.n}_docs_{qs.n}_queries", "docs": docs.n,
                       "nnz": int(docs.nnz), "queries": qs.n, "batch": SQ_BATCH,
                       "query_nnz": "uniform 5-200", "lambda": 6000, "beta": 600, "alpha": 0.4,
-                      "cut": SQ_CUT, "k": K, "heap_factor": head["heap_factor"],
+                      "cut": head["cut"], "k": K, "heap_factor": head["heap_factor"],
                       "l2": "flushed between passes; index > L2",
                       "kernel_variant": args.variant, "kernel_tuning": args.tuning},
-           "build_s": build_s, "sweep": sweep, "peak_gbs": peak, "peak_source": peak_kind}
+           "build_s": build_s, "sweep": sweep, "serving": serving, "peak_gbs": peak,
+           "peak_source": peak_kind}
     print(json.dumps(out))
+
+
+def run_engine_brutal(args):
+    """BrutalIndex exact search at 100k docs, 1,000 queries, k=10 (the
+    CPU-runnable workload): the host-buffer API end to end, the kernel's own
+    time, and the reference's CPU search of the same queries beside it."""
+    import torch
+    torch.cuda.set_device(0)
+    import nsparse
+    from nsparse_b200 import synth
+    n_docs = args.docs if args.docs != N_DOCS else 100_000
+    n_q = args.queries if args.queries != N_QUERIES else 1000
+    docs = synth.docs_config0(n_docs, seed=0)
+    qs = synth.queries_config0(n_q, seed=0)
+    idx = nsparse.index_factory(docs.dim, "brutal")
+    idx.add(docs.n, docs.indptr, docs.indices, docs.values)
+    for _ in range(max(args.warmup, 3)):
+        idx.search(qs.n, qs.indptr, qs.indices, qs.values, K)
+    times, kms = [], []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        D, L = idx.search(qs.n, qs.indptr, qs.indices, qs.values, K)
+        times.append(time.perf_counter() - t)
+        kms.append(nsparse.last_search_stats().kernel_ms)
+    value = qs.n * len(times) / sum(times)
+    kernel_ms = statistics.median(kms)
+    bytes_ = 4 * (docs.n + 1) + 6 * docs.nnz  # forward index read once per launch
+    cpu = None
+    variant = ref_variant()
+    if variant is not None and not args.no_cpu:
+        import oracle as O
+        O.ref_lib(variant).ref_set_threads(os.cpu_count())
+        r = O.RefIndex(docs.dim, "brutal", variant=variant)
+        r.add(docs)
+        sample = qs.rows(0, min(qs.n, 200))
+        r.search(sample.rows(0, 8), K)
+        t = time.perf_counter()
+        r.search(sample, K)
+        dt = time.perf_counter() - t
+        r.close()
+        cpu = {"value": sample.n / dt, "unit": "queries/s", "cores": os.cpu_count(),
+               "kind": "reference",
+               "sample": f"{sample.n} of the {qs.n} queries, reference {variant} build"}
+    print(json.dumps({
+        "metric": "QPS (BrutalIndex exact, 100k docs)", "value": value, "unit": "queries/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
+        "ms_per_step": 1000 * sum(times) / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"brutal_fp32_{docs.n}_docs_{qs.n}_queries", "k": K},
+        "kernel_ms_per_launch": kernel_ms,
+        "kernel_queries_per_s": qs.n / (kernel_ms / 1000.0),
+        "forward_index_gbs": bytes_ / (kernel_ms / 1000.0) / 1e9,
+        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step":
+                4 * (qs.n + 1) + 6 * qs.nnz, "d2h_bytes_per_step": qs.n * K * 8},
+        "cpu_baseline": cpu}))
+
+
+def serve_sweep(nsparse, idx, docs, qs, cut, hf, rates, seconds=2.0):
+    """Serving loop under Poisson arrivals: per offered rate, ~`seconds` of
+    requests (k 10 or 100 at random, 30% carrying a doc filter that admits a
+    random 10% of the docs, labels as random 64-bit external ids); p50/p99
+    latency from scheduled arrival to completion, and the completed rate."""
+    rng = np.random.default_rng(7)
+    srv = nsparse.Server(idx, max_batch=2048, slots=3)
+    srv.set_external_ids(rng.integers(1 << 40, 1 << 62, docs.n, dtype=np.int64))
+    bits = np.zeros((docs.n + 64) // 64, dtype=np.uint64)
+    ids = rng.choice(docs.n, docs.n // 10, replace=False).astype(np.int64)
+    np.bitwise_or.at(bits, ids >> 6, np.left_shift(np.uint64(1), (ids & 63).astype(np.uint64)))
+    fid = srv.add_filter(bits)
+    out = []
+    for rate in rates:
+        n = int(min(qs.n, max(200, rate * seconds)))
+        q = qs.rows(0, n)
+        k_per = np.where(rng.random(n) < 0.5, 10, 100).astype(np.int32)
+        fper = np.where(rng.random(n) < 0.3, fid, -1).astype(np.int32)
+        arrivals = np.cumsum(rng.exponential(1e6 / rate, n))
+        t = time.perf_counter()
+        _, _, lat = srv.replay(q.indptr, q.indices, q.values, k_per, arrivals, cut=cut,
+                               heap_factor=hf, filter_per=fper)
+        wall = time.perf_counter() - t
+        st = srv.stats()
+        lat_ms = np.sort(lat) / 1000.0
+        out.append({"offered_qps": rate, "requests": n, "completed_qps": n / wall,
+                    "p50_ms": float(np.percentile(lat_ms, 50)),
+                    "p99_ms": float(np.percentile(lat_ms, 99)),
+                    "max_batch": st["max_batch"]})
+        log(json.dumps(out[-1]))
+    srv.close()
+    return {"cut": cut, "heap_factor": hf, "slots": 3, "max_batch": 2048, "rates": out}
 
 
 def main():
@@ -516,8 +623,12 @@ def main():
     ap.add_argument("--tuning", type=int, default=0, help="the kernel's tuning value (0: default)")
     ap.add_argument("--kernel-only", action="store_true",
                     help="time the device-resident search launches only and exit")
-    ap.add_argument("--workload", default="fp32-1m", choices=["fp32-1m", "sq8-8.8m"],
-                    help="fp32-1m: the headline workload; sq8-8.8m: SEISMIC-SQ at 8.8M docs")
+    ap.add_argument("--serve-rates", default="5000,20000,50000,100000,200000",
+                    type=lambda s: [float(x) for x in s.split(",") if x],
+                    help="offered request rates (queries/s) for the serving sweep")
+    ap.add_argument("--workload", default="fp32-1m", choices=["fp32-1m", "sq8-8.8m", "brutal-100k"],
+                    help="fp32-1m: the headline workload; sq8-8.8m: SEISMIC-SQ at 8.8M docs "
+                         "with the serving sweep; brutal-100k: exact brute force")
     args = ap.parse_args()
     if (args.docs, args.queries) != (N_DOCS, N_QUERIES):
         N_DOCS, N_QUERIES = args.docs, args.queries
@@ -525,6 +636,8 @@ def main():
                         queries=N_QUERIES)
     if args.workload == "sq8-8.8m":
         run_engine_sq(args)
+    elif args.workload == "brutal-100k":
+        run_engine_brutal(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

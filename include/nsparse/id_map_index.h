@@ -30,6 +30,7 @@ public:
     void add_with_ids(idx_t n, const idx_t* indptr, const term_t* indices, const float* values,
                       const idx_t* ids) override;
     Index* delegate() { return delegate_.get(); }
+    const std::vector<idx_t>& internal_to_external() const { return internal_to_external_; }
 
     void write_index(IOWriter* writer);
     void read_index(IOReader* reader, int io_flags = 0);

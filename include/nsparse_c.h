@@ -196,6 +196,50 @@ nsp_status_t nsp_index_autotune(nsp_index_t* index, int32_t n, const int32_t* in
                                 const nsp_search_params_t* params, int* variant, int* batch_docs,
                                 int* warps_per_block, float* kernel_ms);
 
+/* ---- serving loop (extension with no counterpart in the reference) ------
+ * Single-query requests, each with its own k and an optional doc filter, are
+ * batched continuously: `slots` worker threads (one CUDA stream each) take
+ * whatever requests are waiting when they are free -- those sharing the
+ * oldest request's k, cut and heap factor, up to max_batch, within the
+ * scratch budget -- and run them as one launch, so batches overlap on the GPU.
+ * A request's result equals a search of that query alone. The index (a
+ * seismic index, or an IDMapIndex over one) must outlive the server and stay
+ * unchanged while it runs. */
+typedef struct nsp_server nsp_server_t;
+typedef struct {
+    int32_t max_batch;             /* queries per launch (0: 4096) */
+    int32_t slots;                 /* launches in flight (0: 3) */
+    int64_t scratch_budget_bytes;  /* request bytes in flight (0: 256 MiB) */
+} nsp_server_config_t;
+nsp_status_t nsp_server_new(nsp_index_t* index, const nsp_server_config_t* config,
+                            nsp_server_t** out);
+nsp_status_t nsp_server_free(nsp_server_t* server);
+/* A doc filter: bitmap over internal doc ids (bit d of word d/64), at least
+ * (n_docs + 64) / 64 words, copied to the device once. */
+nsp_status_t nsp_server_add_filter(nsp_server_t* server, const uint64_t* bits, int64_t words,
+                                   int32_t* filter_id);
+/* 64-bit labels: result labels become ids[internal doc id]. */
+nsp_status_t nsp_server_set_external_ids(nsp_server_t* server, const int64_t* ids, int64_t n);
+/* filter_id -1: no filter. */
+nsp_status_t nsp_server_submit(nsp_server_t* server, int32_t nnz, const uint16_t* terms,
+                               const float* values, int k, int cut, float heap_factor,
+                               int32_t filter_id, int64_t* ticket);
+/* Blocks until the request is done; writes k results and the latency. */
+nsp_status_t nsp_server_wait(nsp_server_t* server, int64_t ticket, float* distances,
+                             int64_t* labels, double* latency_us);
+/* Trace replay: request i (row i of the CSR batch, k_per[i], filter_per[i]
+ * or none when filter_per is NULL) is submitted arrival_us[i] microseconds
+ * after the call starts; returns when all are done, with k_stride results
+ * per request (padded with -1.0 / -1) and each latency from its scheduled
+ * arrival to its completion. */
+nsp_status_t nsp_server_replay(nsp_server_t* server, int32_t n, const int32_t* indptr,
+                               const uint16_t* indices, const float* values, const int32_t* k_per,
+                               const int32_t* filter_per, const double* arrival_us, int cut,
+                               float heap_factor, int k_stride, float* distances, int64_t* labels,
+                               double* latency_us);
+/* batches, requests, largest batch, most request bytes in flight. */
+nsp_status_t nsp_server_stats(nsp_server_t* server, int64_t* out4);
+
 /* Number of CUDA devices visible and the name of the current one. */
 nsp_status_t nsp_device_info(int32_t* n_devices, char* name, size_t name_len);
 

@@ -3,12 +3,14 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <memory>
 #include <new>
 #include <stdexcept>
 #include <string>
 
 #include "engine.h"
 #include "index_state.h"
+#include "serve.h"
 #include "nsparse/brutal_index.h"
 #include "nsparse/id_map_index.h"
 #include "nsparse/index_factory.h"
@@ -299,6 +301,87 @@ nsp_status_t nsp_index_autotune(nsp_index_t* index, int32_t n, const int32_t* in
         if (batch_docs != nullptr) *batch_docs = c.batch_docs;
         if (warps_per_block != nullptr) *warps_per_block = c.warps_per_block;
         if (kernel_ms != nullptr) *kernel_ms = c.kernel_ms;
+    });
+}
+
+struct nsp_server {
+    std::unique_ptr<nsparse::detail::Server> s;
+};
+
+namespace {
+nsparse::detail::Server& as_server(nsp_server_t* p) {
+    if (p == nullptr || !p->s) throw std::invalid_argument("unexpected nullptr");
+    return *p->s;
+}
+}  // namespace
+
+nsp_status_t nsp_server_new(nsp_index_t* index, const nsp_server_config_t* config,
+                            nsp_server_t** out) {
+    return guarded([&] {
+        if (index == nullptr || out == nullptr) throw std::invalid_argument("unexpected nullptr");
+        detail::ServerConfig c;
+        if (config != nullptr) {
+            if (config->max_batch < 0 || config->slots < 0 || config->scratch_budget_bytes < 0)
+                throw std::invalid_argument("server limits must not be negative");
+            if (config->max_batch > 0) c.max_batch = config->max_batch;
+            if (config->slots > 0) c.slots = config->slots;
+            if (config->scratch_budget_bytes > 0) c.scratch_budget = config->scratch_budget_bytes;
+        }
+        auto h = std::make_unique<nsp_server>();
+        h->s = std::make_unique<detail::Server>(as_index(index), c);
+        *out = h.release();
+    });
+}
+
+nsp_status_t nsp_server_free(nsp_server_t* server) {
+    return guarded([&] { delete server; });
+}
+
+nsp_status_t nsp_server_add_filter(nsp_server_t* server, const uint64_t* bits, int64_t words,
+                                   int32_t* filter_id) {
+    return guarded([&] {
+        const int id = as_server(server).add_filter(bits, words);
+        if (filter_id != nullptr) *filter_id = id;
+    });
+}
+
+nsp_status_t nsp_server_set_external_ids(nsp_server_t* server, const int64_t* ids, int64_t n) {
+    return guarded([&] { as_server(server).set_external_ids(ids, n); });
+}
+
+nsp_status_t nsp_server_submit(nsp_server_t* server, int32_t nnz, const uint16_t* terms,
+                               const float* values, int k, int cut, float heap_factor,
+                               int32_t filter_id, int64_t* ticket) {
+    return guarded([&] {
+        if (ticket == nullptr) throw std::invalid_argument("unexpected nullptr");
+        *ticket = as_server(server).submit(nnz, terms, values, k, cut, heap_factor, filter_id);
+    });
+}
+
+nsp_status_t nsp_server_wait(nsp_server_t* server, int64_t ticket, float* distances,
+                             int64_t* labels, double* latency_us) {
+    return guarded([&] { as_server(server).wait(ticket, distances, labels, latency_us); });
+}
+
+nsp_status_t nsp_server_replay(nsp_server_t* server, int32_t n, const int32_t* indptr,
+                               const uint16_t* indices, const float* values, const int32_t* k_per,
+                               const int32_t* filter_per, const double* arrival_us, int cut,
+                               float heap_factor, int k_stride, float* distances, int64_t* labels,
+                               double* latency_us) {
+    return guarded([&] {
+        as_server(server).replay(n, indptr, indices, values, k_per, filter_per, arrival_us, cut,
+                                 heap_factor, k_stride, distances, labels, latency_us);
+    });
+}
+
+nsp_status_t nsp_server_stats(nsp_server_t* server, int64_t* out4) {
+    return guarded([&] {
+        if (out4 == nullptr) throw std::invalid_argument("unexpected nullptr");
+        const detail::ServerStats st = as_server(server).stats();
+        out4[0] = st.batches;
+        out4[1] = st.requests;
+        out4[2] = st.max_batch;
+        out4[3] = st.max_in_flight_bytes;
     });
 }
 

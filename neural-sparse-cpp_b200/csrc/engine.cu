@@ -516,6 +516,8 @@ void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
                  int32_t* d_lab, cudaStream_t s, Workspace& ws, SearchStats* stats) {
     SeismicSearchArgs args = args_in;
     if (args.variant < 0) args.variant = kDefaultVariant;
+    if (args.d_sel_q != nullptr && args.variant < 2)
+        throw std::invalid_argument("per-query selectors need a one-CTA-per-query kernel variant");
     const int kind = val_kind_of(args.qbits);
     SeismicLaunch a{};
     a.fwd = fwd.view();
@@ -554,6 +556,7 @@ void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
         a.variant = args.variant;
         a.batch_docs = p.batch_docs;
         a.group_lanes = p.group_lanes;
+        a.sel_q = args.d_sel_q;
         a.bscore = static_cast<float*>(ws.dev(
             Workspace::kBScore, static_cast<size_t>(p.blocks) * p.wpb * maxb * sizeof(float)));
         a.order_stride = (maxb + 7) & ~7;

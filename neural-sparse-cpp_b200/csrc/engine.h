@@ -217,6 +217,9 @@ struct SeismicSearchArgs {
                               // 2-5 one CTA per query with 1, 2, 4, 8 lanes per doc
     int stage_bytes = 0;      // staged: bytes per stage buffer (0 = default)
     int batch_docs = 0;       // variants 2-5: candidate docs per batch (0 = default)
+    // variants 2-5: one device doc bitmap per query (a null entry admits every
+    // doc), in device memory; replaces the launch-wide selector
+    const uint64_t* const* d_sel_q = nullptr;
 };
 
 // Host buffers in, host buffers out (the reference-facing path).

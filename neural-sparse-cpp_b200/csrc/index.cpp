@@ -585,19 +585,12 @@ void search_device(Index* index, int32_t n, const int32_t* d_indptr, const uint1
                                a, d_sel, d_out, d_lab, s, nullptr);
 }
 
-nsp::KernelChoice seismic_autotune(Index* index, idx_t n, const idx_t* indptr,
-                                   const term_t* indices, const float* values, int k,
-                                   SearchParameters* params) {
-    throw_if_not_positive(n);
-    throw_if_not_positive(k);
-    throw_if_any_null(indptr, indices, values);
+SeismicState* resolve_seismic(Index* index, SearchParameters* params, int k,
+                              nsp::SeismicSearchArgs& a) {
     if (auto* im = dynamic_cast<IDMapIndex*>(index)) index = im->delegate();
-    SeismicState* st = nullptr;
-    nsp::SeismicSearchArgs a = seismic_args(params, k);
-    if (auto* si = dynamic_cast<SeismicIndex*>(index)) {
-        st = si->state();
-    } else if (auto* qi = dynamic_cast<SeismicScalarQuantizedIndex*>(index)) {
-        st = qi->state();
+    a = seismic_args(params, k);
+    if (auto* si = dynamic_cast<SeismicIndex*>(index)) return si->state();
+    if (auto* qi = dynamic_cast<SeismicScalarQuantizedIndex*>(index)) {
         const auto* sqp = dynamic_cast<const SeismicSQSearchParameters*>(params);
         const ScalarQuantizer& isq = qi->get_scalar_quantizer();
         const ScalarQuantizer qsq =
@@ -606,9 +599,20 @@ nsp::KernelChoice seismic_autotune(Index* index, idx_t n, const idx_t* indptr,
         a.q_vmin = qsq.get_min();
         a.q_scale = qsq.encode_scale();
         a.decode_scale = isq.decode_scale(qsq);
-    } else {
-        throw std::invalid_argument("autotune applies to seismic indexes");
+        return qi->state();
     }
+    throw std::invalid_argument("this operation applies to seismic indexes");
+}
+
+nsp::KernelChoice seismic_autotune(Index* index, idx_t n, const idx_t* indptr,
+                                   const term_t* indices, const float* values, int k,
+                                   SearchParameters* params) {
+    throw_if_not_positive(n);
+    throw_if_not_positive(k);
+    throw_if_any_null(indptr, indices, values);
+    nsp::SeismicSearchArgs a;
+    SeismicState* st = resolve_seismic(index, params, k, a);
+    if (auto* im = dynamic_cast<IDMapIndex*>(index)) index = im->delegate();
     if (st->vectors.host.n() == 0) throw std::runtime_error("index is empty");
     st->vectors.ensure_device();
     st->ensure_lists();

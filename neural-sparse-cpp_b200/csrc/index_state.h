@@ -51,6 +51,15 @@ void seismic_build(SeismicState& st, int dim, const SeismicClusterParameters& pa
 
 std::vector<uint64_t> selector_bitmap(const IDSelector* sel, int64_t n_docs);
 
+// The SEISMIC state behind `index` (an IDMapIndex's delegate too) and the
+// kernel arguments `params` ask for, SQ query encoding included; throws
+// std::invalid_argument for other index types.
+SeismicState* resolve_seismic(Index* index, SearchParameters* params, int k,
+                              nsp::SeismicSearchArgs& a);
+
+// The autotuner's launch shape, where the caller left the choice to the engine.
+void apply_tuned(const SeismicState& st, nsp::SeismicSearchArgs& a);
+
 // Times every one-CTA-per-query launch shape (lanes per doc x batch x warps)
 // on a sample of queries and keeps the fastest for later searches that leave
 // the kernel to the engine (seismic indexes, also through an IDMapIndex).

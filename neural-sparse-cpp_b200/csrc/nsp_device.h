@@ -105,6 +105,7 @@ struct SeismicLaunch {
     // (nullptr when none is).
     int32_t batch_docs;
     int32_t group_lanes;
+    const uint64_t* const* sel_q;  // per-query doc bitmaps (null entry: none), or nullptr
     uint16_t* order;
     int32_t order_stride;
     unsigned long long* sortkeys;
@@ -128,6 +129,20 @@ struct ExactLaunch {
     int32_t* out_l;
     unsigned long long* stats;
 };
+
+// Lets kernel `f` use the device's whole opt-in shared memory. Every call sets
+// the same value, so launches from several host threads cannot undo one
+// another's setting, as a per-launch size could between a set and a launch.
+template <class F>
+inline cudaError_t allow_opt_in_smem(F f) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    int v = 0;
+    e = cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+}
 
 // Launchers (return cudaError_t of the launch). `sm_count` sizes persistent
 // grids; `plan_*` report the dynamic shared memory a launch needs.

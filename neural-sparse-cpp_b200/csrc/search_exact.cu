@@ -301,9 +301,7 @@ cudaError_t launch_exact(const ExactLaunch& a, int tiles, cudaStream_t s) {
     if (a.q.n == 0) return cudaSuccess;
     const int words = (a.fwd.dim + 31) / 32;
     const size_t smem = exact_smem_bytes(words, a.qval_global != nullptr ? 0 : a.qcap);
-    cudaError_t e = cudaFuncSetAttribute(exact_tile_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
+    cudaError_t e = allow_opt_in_smem(exact_tile_kernel);
     if (e != cudaSuccess) return e;
     const int groups = (a.q.n + kQG - 1) / kQG;
     exact_tile_kernel<<<dim3(tiles, groups), kWarps * 32, smem, s>>>(a);

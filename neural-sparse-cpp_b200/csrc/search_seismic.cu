@@ -937,9 +937,7 @@ template <typename V, bool kStaged>
 static int max_blocks_typed(int wpb, size_t smem) {
     // the occupancy calculator only admits dynamic shared memory the kernel
     // has been allowed to use
-    if (cudaFuncSetAttribute(seismic_search_kernel<V, kStaged>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem)) != cudaSuccess)
+    if (allow_opt_in_smem(seismic_search_kernel<V, kStaged>) != cudaSuccess)
         return 0;
     int blocks = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, seismic_search_kernel<V, kStaged>,
@@ -967,9 +965,7 @@ static cudaError_t launch_typed(const SeismicLaunch& a, int wpb, int blocks, cud
     const size_t smem = slice_bytes(static_cast<int>(sizeof(V)), a.ix.words, a.qcap, a.k,
                                     kStaged ? a.bcap : 0, kStaged ? a.stage_bytes : 0) *
                         wpb;
-    cudaError_t e = cudaFuncSetAttribute(seismic_search_kernel<V, kStaged>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
+    cudaError_t e = allow_opt_in_smem(seismic_search_kernel<V, kStaged>);
     if (e != cudaSuccess) return e;
     seismic_search_kernel<V, kStaged><<<blocks, wpb * 32, smem, s>>>(a);
     return cudaGetLastError();
@@ -994,9 +990,7 @@ static cudaError_t launch_exact_list_t(const FwdView& fwd, const QueryView& q, c
                                        float* out_d, int32_t* out_l, cudaStream_t s) {
     const int words = (fwd.dim + 31) / 32;
     const size_t smem = slice_bytes(static_cast<int>(sizeof(V)), words, qcap, k);
-    cudaError_t e = cudaFuncSetAttribute(exact_list_kernel<V>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
+    cudaError_t e = allow_opt_in_smem(exact_list_kernel<V>);
     if (e != cudaSuccess) return e;
     if (q.n == 0) return cudaSuccess;
     exact_list_kernel<V><<<q.n, 32, smem, s>>>(fwd, q, ids, n_ids, k, decode_scale, words, qcap,

@@ -561,6 +561,7 @@ __global__ void __launch_bounds__(256, 4) seismic_cta_kernel(SeismicLaunch a) {
         const int q = ctl->q;
         if (q >= a.q.n) break;
 
+        const uint64_t* sel = a.sel_q != nullptr ? a.sel_q[q] : a.sel_bits;
         // 1. scatter the query
         const int32_t qs = a.q.indptr[q];
         int qn = a.q.indptr[q + 1] - qs;
@@ -685,8 +686,8 @@ __global__ void __launch_bounds__(256, 4) seismic_cta_kernel(SeismicLaunch a) {
                             const Seg& g = segs[lo];
                             const int32_t d = __ldg(a.ix.docs + g.d0 + (i - g.cand0));
                             bool member = true;
-                            if (a.sel_bits != nullptr)
-                                member = (__ldg(a.sel_bits + (d >> 6)) >> (d & 63)) & 1ull;
+                            if (sel != nullptr)
+                                member = (__ldg(sel + (d >> 6)) >> (d & 63)) & 1ull;
                             uint2 ri = make_uint2(0u, 0u);
                             if (member) ri = __ldg(a.fwd.rowinfo + d);
                             cdoc[i] = member ? d : -1;
@@ -802,9 +803,7 @@ size_t smem_typed(int dim, int qcap, int k, int batch) {
 
 template <typename V, typename TE, int kG>
 int max_blocks_cta_g(int threads, size_t smem) {
-    if (cudaFuncSetAttribute(seismic_cta_kernel<V, TE, kG>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem)) != cudaSuccess)
+    if (allow_opt_in_smem(seismic_cta_kernel<V, TE, kG>) != cudaSuccess)
         return 0;
     int blocks = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, seismic_cta_kernel<V, TE, kG>,
@@ -824,9 +823,7 @@ int max_blocks_cta_typed(int group, int threads, size_t smem) {
 template <typename V, typename TE, int kG>
 cudaError_t launch_cta_g(const SeismicLaunch& a, int warps, int blocks, size_t smem,
                          cudaStream_t s) {
-    cudaError_t e = cudaFuncSetAttribute(seismic_cta_kernel<V, TE, kG>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
+    cudaError_t e = allow_opt_in_smem(seismic_cta_kernel<V, TE, kG>);
     if (e != cudaSuccess) return e;
     seismic_cta_kernel<V, TE, kG><<<blocks, warps * 32, smem, s>>>(a);
     return cudaGetLastError();

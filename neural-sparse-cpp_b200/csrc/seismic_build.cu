@@ -554,6 +554,52 @@ __global__ void kept_pairs_kernel(const uint64_t* pkey_sorted, const int64_t* pa
     }
 }
 
+// Per kept summary pair (sorted by (term, block) within each list): its block
+// id, its value as the index stores it, and a flag where a new term starts.
+template <int ESZ>
+__global__ void columns_kernel(const uint32_t* key, const float* val, int64_t n, uint16_t* blk,
+                               uint8_t* out_val, int64_t* flag) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        blk[i] = static_cast<uint16_t>(key[i] & 0xffffu);
+        const float v = val[i];
+        if constexpr (ESZ == 4) {
+            reinterpret_cast<float*>(out_val)[i] = v;
+        } else if constexpr (ESZ == 2) {
+            reinterpret_cast<uint16_t*>(out_val)[i] = static_cast<uint16_t>(v);
+        } else {
+            out_val[i] = static_cast<uint8_t>(v);
+        }
+        flag[i] = (i == 0 || (key[i] >> 16) != (key[i - 1] >> 16)) ? 1 : 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) flag[n] = 0;
+}
+
+// A list's first pair always starts a column (its term may equal the last
+// term of the list before).
+__global__ void list_start_kernel(const int32_t* list_off, int32_t nl, int64_t n, int64_t* flag) {
+    const int32_t l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l < nl && list_off[l] < list_off[l + 1] && list_off[l] < n) flag[list_off[l]] = 1;
+}
+
+__global__ void column_compact_kernel(const uint32_t* key, const int64_t* flag, const int64_t* pos,
+                                      int64_t n, uint16_t* term, int64_t* start) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        if (flag[i]) {
+            term[pos[i]] = static_cast<uint16_t>(key[i] >> 16);
+            start[pos[i]] = i;
+        }
+    }
+}
+
+// Columns before each list boundary.
+__global__ void list_cols_kernel(const int32_t* list_off, int32_t nl, const int64_t* pos,
+                                 int64_t* cols) {
+    const int32_t l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l <= nl) cols[l] = pos[list_off[l]];
+}
+
 template <int ESZ>
 void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
                      const DevArray<int64_t>& d_bdp, nsp::SeismicHost& L, int32_t t0, int32_t t1,
@@ -662,31 +708,45 @@ void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
     to_dev(d_list_koff, to_i32_offsets(list_koff), s);
     segmented_sort_pairs(tkey.data(), tkey2.data(), tval.data(), tval2.data(), n_kept, t1 - t0,
                          d_list_koff.data(), s, /*stable=*/false);
-    const std::vector<uint32_t> hk = to_host(tkey2, static_cast<size_t>(n_kept), s);
-    const std::vector<float> hv = to_host(tval2, static_cast<size_t>(n_kept), s);
-    for (int32_t t = t0; t < t1; ++t) {
-        const int64_t k0 = list_koff[t - t0], k1 = list_koff[t - t0 + 1];
-        for (int64_t i = k0; i < k1; ++i) {
-            const uint16_t term = static_cast<uint16_t>(hk[i] >> 16);
-            if (i == k0 || term != static_cast<uint16_t>(hk[i - 1] >> 16)) {
-                L.sterm.push_back(term);
-                L.srun.push_back(L.srun.back());
-            }
-            L.srun.back() += 1;
-            L.sblk.push_back(static_cast<uint16_t>(hk[i] & 0xffffu));
-            if constexpr (ESZ == 4) {
-                const uint8_t* b = reinterpret_cast<const uint8_t*>(&hv[i]);
-                L.sval.insert(L.sval.end(), b, b + 4);
-            } else if constexpr (ESZ == 2) {
-                const uint16_t c = static_cast<uint16_t>(hv[i]);
-                const uint8_t* b = reinterpret_cast<const uint8_t*>(&c);
-                L.sval.insert(L.sval.end(), b, b + 2);
-            } else {
-                L.sval.push_back(static_cast<uint8_t>(hv[i]));
-            }
-        }
-        L.ltp.push_back(static_cast<int64_t>(L.sterm.size()));
-    }
+    // columns assembled on the device: block ids, values, and one run per
+    // (list, term) with its start
+    const int32_t nl = t1 - t0;
+    DevArray<uint16_t> o_blk(std::max<int64_t>(n_kept, 1));
+    DevArray<uint8_t> o_val(std::max<int64_t>(n_kept, 1) * ESZ);
+    DevArray<int64_t> rflag(static_cast<size_t>(n_kept) + 1), rpos(static_cast<size_t>(n_kept) + 1);
+    columns_kernel<ESZ><<<sms * 8, 256, 0, s>>>(tkey2.data(), tval2.data(), n_kept, o_blk.data(),
+                                                o_val.data(), rflag.data());
+    cuda_check(cudaGetLastError(), "columns_kernel");
+    list_start_kernel<<<std::max(1, (nl + 255) / 256), 256, 0, s>>>(d_list_koff.data(), nl,
+                                                                    n_kept, rflag.data());
+    cuda_check(cudaGetLastError(), "list_start_kernel");
+    nsp::exclusive_scan_i64(rflag.data(), rpos.data(), n_kept + 1, s);
+    int64_t n_cols = 0;
+    cuda_check(cudaMemcpyAsync(&n_cols, rpos.data() + n_kept, 8, cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    DevArray<uint16_t> o_term(std::max<int64_t>(n_cols, 1));
+    DevArray<int64_t> o_start(std::max<int64_t>(n_cols, 1)), o_lcol(static_cast<size_t>(nl) + 1);
+    column_compact_kernel<<<sms * 8, 256, 0, s>>>(tkey2.data(), rflag.data(), rpos.data(), n_kept,
+                                                  o_term.data(), o_start.data());
+    cuda_check(cudaGetLastError(), "column_compact_kernel");
+    list_cols_kernel<<<std::max(1, (nl + 1 + 255) / 256), 256, 0, s>>>(d_list_koff.data(), nl,
+                                                                       rpos.data(), o_lcol.data());
+    cuda_check(cudaGetLastError(), "list_cols_kernel");
+    const std::vector<uint16_t> h_blk = to_host(o_blk, static_cast<size_t>(n_kept), s);
+    const std::vector<uint8_t> h_val = to_host(o_val, static_cast<size_t>(n_kept) * ESZ, s);
+    const std::vector<uint16_t> h_term = to_host(o_term, static_cast<size_t>(n_cols), s);
+    const std::vector<int64_t> h_start = to_host(o_start, static_cast<size_t>(n_cols), s);
+    const std::vector<int64_t> h_lcol = to_host(o_lcol, static_cast<size_t>(nl) + 1, s);
+    const int64_t ebase = static_cast<int64_t>(L.sblk.size());
+    const int64_t cbase = static_cast<int64_t>(L.sterm.size());
+    L.sblk.insert(L.sblk.end(), h_blk.begin(), h_blk.end());
+    L.sval.insert(L.sval.end(), h_val.begin(), h_val.end());
+    L.sterm.insert(L.sterm.end(), h_term.begin(), h_term.end());
+    // srun holds column boundaries: the first column starts where the last
+    // batch ended (srun.back() == ebase)
+    for (int64_t c = 1; c < n_cols; ++c) L.srun.push_back(ebase + h_start[c]);
+    if (n_cols > 0) L.srun.push_back(ebase + n_kept);
+    for (int32_t l = 0; l < nl; ++l) L.ltp.push_back(cbase + h_lcol[l + 1]);
 }
 
 // Phase timings on stderr when NSP_VERBOSE=1 (the engine's one debug switch).

@@ -389,3 +389,102 @@ def device_info():
     buf = ctypes.create_string_buffer(256)
     _check(_L.nsp_device_info(ctypes.byref(n), buf, 256))
     return n.value, buf.value.decode()
+
+
+# ------------------------------------------------------------ serving ----
+
+class _ServerConfig(ctypes.Structure):
+    _fields_ = [("max_batch", ctypes.c_int32), ("slots", ctypes.c_int32),
+                ("scratch_budget_bytes", ctypes.c_int64)]
+
+
+_sig("nsp_server_new", _P, ctypes.POINTER(_ServerConfig), ctypes.POINTER(_P))
+_sig("nsp_server_free", _P)
+_sig("nsp_server_add_filter", _P, _P, ctypes.c_int64, ctypes.POINTER(_I32))
+_sig("nsp_server_set_external_ids", _P, _P, ctypes.c_int64)
+_sig("nsp_server_submit", _P, _I32, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_float, _I32,
+     ctypes.POINTER(ctypes.c_int64))
+_sig("nsp_server_wait", _P, ctypes.c_int64, _P, _P, ctypes.POINTER(ctypes.c_double))
+_sig("nsp_server_replay", _P, _I32, _P, _P, _P, _P, _P, _P, ctypes.c_int, ctypes.c_float,
+     ctypes.c_int, _P, _P, _P)
+_sig("nsp_server_stats", _P, ctypes.POINTER(ctypes.c_int64))
+
+
+class Server:
+    """Extension: continuous-batching serving loop over a seismic index (or an
+    IDMapIndex over one). Single-query requests with their own k and optional
+    doc filter are batched by the engine as they arrive; each result equals a
+    search of that query alone. Keep the index alive and unchanged while the
+    server runs."""
+
+    def __init__(self, index, max_batch=0, slots=0, scratch_budget_bytes=0):
+        self._index = index
+        cfg = _ServerConfig(int(max_batch), int(slots), int(scratch_budget_bytes))
+        h = _P()
+        _check(_L.nsp_server_new(index._h, ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h.value
+
+    def add_filter(self, bits):
+        """A doc filter: uint64 bitmap over internal doc ids. Returns its id."""
+        bits = np.ascontiguousarray(bits, dtype=np.uint64)
+        out = _I32()
+        _check(_L.nsp_server_add_filter(self._h, _ptr(bits), bits.size, ctypes.byref(out)))
+        return out.value
+
+    def set_external_ids(self, ids):
+        ids = np.ascontiguousarray(ids, dtype=np.int64)
+        _check(_L.nsp_server_set_external_ids(self._h, _ptr(ids), ids.size))
+
+    def submit(self, terms, values, k=10, cut=10, heap_factor=1.0, filter_id=-1):
+        terms = np.ascontiguousarray(terms, dtype=np.uint16)
+        values = np.ascontiguousarray(values, dtype=np.float32)
+        t = ctypes.c_int64()
+        _check(_L.nsp_server_submit(self._h, terms.size, _ptr(terms), _ptr(values), int(k),
+                                    int(cut), float(heap_factor), int(filter_id), ctypes.byref(t)))
+        return t.value, int(k)
+
+    def wait(self, ticket):
+        """ticket: what submit() returned. Returns (distances, labels, latency_us)."""
+        t, k = ticket
+        d = np.empty(k, dtype=np.float32)
+        l = np.empty(k, dtype=np.int64)
+        lat = ctypes.c_double()
+        _check(_L.nsp_server_wait(self._h, t, _ptr(d), _ptr(l), ctypes.byref(lat)))
+        return d, l, lat.value
+
+    def replay(self, indptr, indices, values, k_per, arrival_us, cut=10, heap_factor=1.0,
+               filter_per=None):
+        """Submits row i at arrival_us[i] (microseconds from the call) and waits
+        for all. Returns (distances, labels, latency_us), max(k_per) per row."""
+        indptr = np.ascontiguousarray(indptr, dtype=np.int32)
+        indices = np.ascontiguousarray(indices, dtype=np.uint16)
+        values = np.ascontiguousarray(values, dtype=np.float32)
+        k_per = np.ascontiguousarray(k_per, dtype=np.int32)
+        arrival_us = np.ascontiguousarray(arrival_us, dtype=np.float64)
+        n = len(indptr) - 1
+        ks = int(k_per.max())
+        fp = None if filter_per is None else np.ascontiguousarray(filter_per, dtype=np.int32)
+        d = np.empty((n, ks), dtype=np.float32)
+        l = np.empty((n, ks), dtype=np.int64)
+        lat = np.empty(n, dtype=np.float64)
+        _check(_L.nsp_server_replay(self._h, n, _ptr(indptr), _ptr(indices), _ptr(values),
+                                    _ptr(k_per), _ptr(fp), _ptr(arrival_us), int(cut),
+                                    float(heap_factor), ks, _ptr(d), _ptr(l), _ptr(lat)))
+        return d, l, lat
+
+    def stats(self):
+        out = (ctypes.c_int64 * 4)()
+        _check(_L.nsp_server_stats(self._h, out))
+        return {"batches": out[0], "requests": out[1], "max_batch": out[2],
+                "max_in_flight_bytes": out[3]}
+
+    def close(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            _L.nsp_server_free(h)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
