@@ -117,7 +117,8 @@ nsp_status_t nsp_seismic_sq_search_params_new(float vmin, float vmax, int cut,
 nsp_status_t nsp_search_params_set_id_selector(nsp_search_params_t* params,
                                                nsp_id_selector_t* sel);
 /* Extension: plain = 1 runs one kernel launch per query instead of one
- * batched launch; warps_per_block = 0 lets the engine choose. */
+ * batched launch; warps_per_block (1-32; the warp-per-query variants 0-1 use
+ * at most 8) = 0 lets the engine choose. */
 nsp_status_t nsp_search_params_set_engine(nsp_search_params_t* params, int plain,
                                           int warps_per_block);
 /* Extension: SEISMIC kernel variant (-1 engine's choice, 0 one warp per query

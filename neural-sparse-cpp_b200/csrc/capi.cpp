@@ -232,9 +232,9 @@ nsp_status_t nsp_search_params_set_engine(nsp_search_params_t* params, int plain
                                           int warps_per_block) {
     return guarded([&] {
         if (params == nullptr) throw std::invalid_argument("unexpected nullptr");
-        if (warps_per_block < 0 || warps_per_block > 8)
-            throw std::invalid_argument("warps_per_block must be in [0, 8]");
         as_params(params)->engine.plain = plain != 0;
+        if (warps_per_block < 0 || warps_per_block > 32)
+            throw std::invalid_argument("warps_per_block must be in [0, 32]");
         as_params(params)->engine.warps_per_block = warps_per_block;
     });
 }

@@ -452,15 +452,26 @@ struct SeismicPlan {
     int group_lanes;  // variants 2-5: lanes per scored doc
 };
 
-// Variants 2-5 (one CTA per query): 8 warps and batches of 512 candidate docs
-// unless asked otherwise; the batch shrinks if shared memory is short.
+// Variants 2-5 (one CTA per query). Warps per CTA: 8 when the batch has
+// queries enough to give every SM four CTAs; fewer queries get bigger CTAs
+// (16 or 32 warps, up to a whole SM per query), which shortens each query's
+// sequence of candidate batches -- the latency of small batches and of the
+// one-query-per-launch path. Candidate docs per batch: 64 per warp unless
+// asked otherwise; the batch shrinks if shared memory is short.
 SeismicPlan plan_seismic_cta(int kind, int dim, int qcap, int k, int n_queries,
                              const SeismicSearchArgs& args, bool single) {
     SeismicPlan p{};
     p.variant = args.variant;
-    int warps = args.warps_per_block > 0 ? args.warps_per_block : 8;
-    warps = std::min(std::max(warps, 1), 8);
-    int batch = args.batch_docs > 0 ? args.batch_docs : 512;
+    int warps = args.warps_per_block;
+    if (warps <= 0) {
+        const int sms = device_sm_count();
+        const int per = single ? 1 : std::max(n_queries, 1);
+        warps = 8;
+        if (per * 2 <= sms) warps = 32;
+        else if (per <= 2 * sms) warps = 16;
+    }
+    warps = std::min(std::max(warps, 1), 32);
+    int batch = args.batch_docs > 0 ? args.batch_docs : 64 * warps;
     batch = std::min(std::max((batch + 31) & ~31, 32), 8192);
     const size_t limit = static_cast<size_t>(max_smem_optin());
     while (batch > 32 && seismic_cta_smem(kind, dim, qcap, k, batch) > limit) batch >>= 1;
@@ -496,7 +507,8 @@ SeismicPlan plan_seismic(int kind, int words, int qcap, int k, int n_queries,
     const size_t limit = static_cast<size_t>(max_smem_optin());
     if (p.smem_per_warp > limit)
         throw std::invalid_argument("query too long or k too large for the device search kernel");
-    int wpb = args.warps_per_block > 0 ? args.warps_per_block : (p.variant == 1 ? 2 : 4);
+    int wpb = args.warps_per_block > 0 ? std::min(args.warps_per_block, 8)
+                                       : (p.variant == 1 ? 2 : 4);
     while (wpb > 1 && p.smem_per_warp * wpb > limit) wpb >>= 1;
     p.wpb = wpb;
     int per_sm = seismic_max_blocks_per_sm(kind, p.variant, wpb, p.smem_per_warp * wpb);

@@ -511,7 +511,7 @@ __device__ int gather(const SeismicLaunch& a, Cursor& c, bool first, int64_t lb0
 }
 
 template <typename V, typename TE, int kG>
-__global__ void __launch_bounds__(256, 4) seismic_cta_kernel(SeismicLaunch a) {
+__global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr bool kRank = std::is_same<V, float>::value;
     constexpr int vsz = static_cast<int>(sizeof(V));

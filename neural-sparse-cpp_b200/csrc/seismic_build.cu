@@ -39,6 +39,8 @@
 #include <cstdint>
 #include <cstring>
 #include <random>
+#include <utility>
+#include <string>
 #include <stdexcept>
 #include <thread>
 #include <vector>
@@ -600,6 +602,41 @@ __global__ void list_cols_kernel(const int32_t* list_off, int32_t nl, const int6
     if (l <= nl) cols[l] = pos[list_off[l]];
 }
 
+// Time per step of the summary pipeline, summed over batches, on stderr when
+// NSP_VERBOSE=1 (the engine's one debug switch; it synchronizes each step).
+struct StepTimes {
+    bool on = false;
+    cudaStream_t s = nullptr;
+    std::chrono::steady_clock::time_point t;
+    std::vector<std::pair<std::string, double>> acc;
+    void start(cudaStream_t st) {
+        const char* v = std::getenv("NSP_VERBOSE");
+        on = v != nullptr && v[0] == '1';
+        s = st;
+        acc.clear();
+        t = std::chrono::steady_clock::now();
+    }
+    void mark(const char* name) {
+        if (!on) return;
+        cudaStreamSynchronize(s);
+        const auto now = std::chrono::steady_clock::now();
+        const double dt = std::chrono::duration<double>(now - t).count();
+        t = now;
+        for (auto& a : acc)
+            if (a.first == name) {
+                a.second += dt;
+                return;
+            }
+        acc.emplace_back(name, dt);
+    }
+    void print() const {
+        if (!on) return;
+        for (const auto& a : acc)
+            std::fprintf(stderr, "[nsparse build]   %-14s %8.3f s\n", a.first.c_str(), a.second);
+    }
+};
+thread_local StepTimes g_steps;
+
 template <int ESZ>
 void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
                      const DevArray<int64_t>& d_bdp, nsp::SeismicHost& L, int32_t t0, int32_t t1,
@@ -620,6 +657,7 @@ void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
                                                 d_doc_eoff.data(), e0, ekey.data(), eidx.data(),
                                                 eval.data());
     cuda_check(cudaGetLastError(), "entries_kernel");
+    g_steps.mark("entries");
     std::vector<int64_t> boff64(blk_e.begin() + b0, blk_e.begin() + b1 + 1);
     for (auto& v : boff64) v -= e0;
     DevArray<int32_t> d_boff;
@@ -629,6 +667,7 @@ void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
                          d_boff.data(), s, /*stable=*/true);
     ekey.reset();
     eidx.reset();
+    g_steps.mark("sort entries");
     DevArray<int32_t> entry_block(ne);
     fill_block_kernel<<<sms * 8, 256, 0, s>>>(d_boff.data(), nb, entry_block.data());
     cuda_check(cudaGetLastError(), "fill_block_kernel");
@@ -641,6 +680,7 @@ void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
     cuda_check(cudaMemcpyAsync(&last_flag, flag.data() + ne - 1, 8, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaStreamSynchronize(s), "sync");
     const int64_t n_runs = last_pos + last_flag;
+    g_steps.mark("runs scan");
     DevArray<int32_t> run_start(n_runs);
     run_compact_kernel<<<sms * 8, 256, 0, s>>>(flag.data(), pos.data(), ne, run_start.data());
     cuda_check(cudaGetLastError(), "run_compact_kernel");
@@ -672,12 +712,14 @@ void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
     mass_kernel<<<sms * 4, 128, 0, s>>>(delta.data(), has_delta.data(), d_boff.data(), nb,
                                         mass.data());
     cuda_check(cudaGetLastError(), "mass_kernel");
+    g_steps.mark("runs, mass");
     // alpha cut over each block's maxima, value descending
     DevArray<int32_t> d_pair_off32;
     to_dev(d_pair_off32, to_i32_offsets(pair_off), s);
     segmented_sort_keys(pkey.data(), pkey2.data(), n_runs, nb, d_pair_off32.data(), s);
     DevArray<int64_t> d_pair_off;
     to_dev(d_pair_off, pair_off, s);
+    g_steps.mark("sort maxima");
     DevArray<int32_t> keep(nb);
     cut_kernel<<<sms * 4, 128, 0, s>>>(pkey2.data(), d_pair_off.data(), nb, mass.data(), alpha,
                                        keep.data());
@@ -703,11 +745,13 @@ void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
                                               d_kept_off.data(), d_block_local.data(), nb,
                                               tkey.data(), tval.data());
     cuda_check(cudaGetLastError(), "kept_pairs_kernel");
+    g_steps.mark("alpha cut");
     // term-major per list (build_transpose, inverted_list_clusters.cpp:230-293)
     DevArray<int32_t> d_list_koff;
     to_dev(d_list_koff, to_i32_offsets(list_koff), s);
     segmented_sort_pairs(tkey.data(), tkey2.data(), tval.data(), tval2.data(), n_kept, t1 - t0,
                          d_list_koff.data(), s, /*stable=*/false);
+    g_steps.mark("transpose sort");
     // columns assembled on the device: block ids, values, and one run per
     // (list, term) with its start
     const int32_t nl = t1 - t0;
@@ -737,6 +781,7 @@ void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
     const std::vector<uint16_t> h_term = to_host(o_term, static_cast<size_t>(n_cols), s);
     const std::vector<int64_t> h_start = to_host(o_start, static_cast<size_t>(n_cols), s);
     const std::vector<int64_t> h_lcol = to_host(o_lcol, static_cast<size_t>(nl) + 1, s);
+    g_steps.mark("columns, D2H");
     const int64_t ebase = static_cast<int64_t>(L.sblk.size());
     const int64_t cbase = static_cast<int64_t>(L.sterm.size());
     L.sblk.insert(L.sblk.end(), h_blk.begin(), h_blk.end());
@@ -747,6 +792,7 @@ void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
     for (int64_t c = 1; c < n_cols; ++c) L.srun.push_back(ebase + h_start[c]);
     if (n_cols > 0) L.srun.push_back(ebase + n_kept);
     for (int32_t l = 0; l < nl; ++l) L.ltp.push_back(cbase + h_lcol[l + 1]);
+    g_steps.mark("host append");
 }
 
 // Phase timings on stderr when NSP_VERBOSE=1 (the engine's one debug switch).
@@ -949,6 +995,7 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
     DevArray<int32_t> d_docs;
     to_dev(d_docs, L.docs, s);
     const int64_t budget = int64_t{1} << 27;  // entries per batch
+    g_steps.start(s);
     L.ltp.assign(1, 0);
     L.srun.assign(1, 0);
     L.sterm.clear();
@@ -971,6 +1018,7 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
     }
 
     clock.mark("summaries");
+    g_steps.print();
     // ---- 6. publish
     std::lock_guard<std::mutex> g(st.mu);
     st.lists = std::move(L);

@@ -113,8 +113,7 @@ int64_t Server::submit(int32_t nnz, const uint16_t* terms, const float* values, 
     r->ticket = next_ticket_++;
     r->t_arrive = Clock::now();
     live_[r->ticket] = r;
-    pending_.push_back(r);
-    cv_work_.notify_one();
+    enqueue(r);
     return r->ticket;
 }
 
@@ -169,8 +168,7 @@ void Server::replay(int32_t n, const int32_t* indptr, const uint16_t* indices, c
         std::lock_guard<std::mutex> g(mu_);
         reqs[i]->ticket = next_ticket_++;
         reqs[i]->t_arrive = at;  // latency counts from the scheduled arrival
-        pending_.push_back(reqs[i]);
-        cv_work_.notify_one();
+        enqueue(reqs[i]);
     }
     {
         std::unique_lock<std::mutex> lk(mu_);
@@ -193,6 +191,17 @@ void Server::replay(int32_t n, const int32_t* indptr, const uint16_t* indices, c
     }
 }
 
+// Requests wait in one queue per (k, cut, heap factor): a launch serves one
+// such combination, and taking a batch never scans other requests.
+void Server::enqueue(const std::shared_ptr<ServerRequest>& r) {
+    uint32_t hf_bits = 0;
+    std::memcpy(&hf_bits, &r->hf, sizeof(hf_bits));
+    const QueueKey key{r->k, r->cut, hf_bits};
+    pending_[key].push_back(r);
+    ++n_pending_;
+    cv_work_.notify_one();
+}
+
 ServerStats Server::stats() const {
     std::lock_guard<std::mutex> g(mu_);
     return stats_;
@@ -208,28 +217,28 @@ void Server::worker() {
         {
             std::unique_lock<std::mutex> lk(mu_);
             cv_work_.wait(lk, [&] {
-                return stop_ || (!pending_.empty() && in_use_ < cfg_.scratch_budget);
+                return stop_ || (n_pending_ > 0 && in_use_ < cfg_.scratch_budget);
             });
-            if (pending_.empty()) {
+            if (n_pending_ == 0) {
                 if (stop_) return;
                 continue;
             }
-            const ServerRequest& head = *pending_.front();
-            const int k = head.k, cut = head.cut;
-            const float hf = head.hf;
-            for (auto it = pending_.begin();
-                 it != pending_.end() && static_cast<int>(batch.size()) < cfg_.max_batch;) {
-                const ServerRequest& r = **it;
-                if (r.k == k && r.cut == cut && r.hf == hf) {
-                    const int64_t e = request_bytes(r);
-                    if (!batch.empty() && in_use_ + est + e > cfg_.scratch_budget) break;
-                    est += e;
-                    batch.push_back(*it);
-                    it = pending_.erase(it);
-                } else {
-                    ++it;
-                }
+            // the queue (one per k, cut, heap factor) whose head waited longest
+            auto q = pending_.end();
+            for (auto it = pending_.begin(); it != pending_.end(); ++it)
+                if (!it->second.empty() &&
+                    (q == pending_.end() ||
+                     it->second.front()->t_arrive < q->second.front()->t_arrive))
+                    q = it;
+            auto& dq = q->second;
+            while (!dq.empty() && static_cast<int>(batch.size()) < cfg_.max_batch) {
+                const int64_t e = request_bytes(*dq.front());
+                if (!batch.empty() && in_use_ + est + e > cfg_.scratch_budget) break;
+                est += e;
+                batch.push_back(dq.front());
+                dq.pop_front();
             }
+            n_pending_ -= static_cast<int64_t>(batch.size());
             in_use_ += est;
             sel.assign(batch.size(), nullptr);
             for (size_t i = 0; i < batch.size(); ++i)

@@ -7,6 +7,8 @@
 #include <condition_variable>
 #include <cstdint>
 #include <deque>
+#include <map>
+#include <tuple>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -80,6 +82,16 @@ private:
                                                 int filter) const;
     int index_dimension() const;
     void worker();
+    void enqueue(const std::shared_ptr<ServerRequest>& r);  // under mu_
+
+    struct QueueKey {
+        int k;
+        int cut;
+        uint32_t hf_bits;
+        bool operator<(const QueueKey& o) const {
+            return std::tie(k, cut, hf_bits) < std::tie(o.k, o.cut, o.hf_bits);
+        }
+    };
 
     Index* index_;
     ServerConfig cfg_;
@@ -92,7 +104,8 @@ private:
 
     mutable std::mutex mu_;
     std::condition_variable cv_work_, cv_done_;
-    std::deque<std::shared_ptr<ServerRequest>> pending_;
+    std::map<QueueKey, std::deque<std::shared_ptr<ServerRequest>>> pending_;
+    int64_t n_pending_ = 0;
     std::unordered_map<int64_t, std::shared_ptr<ServerRequest>> live_;
     int64_t next_ticket_ = 0;
     int64_t in_use_ = 0;

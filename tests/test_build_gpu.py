@@ -162,6 +162,52 @@ def test_sq_build_assignment_and_summaries_match_reference(tmp_path):
     assert checked > 50
 
 
+def test_sq_build_full_size_lists_match_reference_assigner(tmp_path):
+    """The 8.8M-doc build's list shape at 1M docs: postings capped at 6,000 and
+    600 blocks per full list (uint8 codes, config-2 generator). For the 12
+    longest lists and 12 other full ones, the reference's assigner, given the engine's kept list and
+    centroids, produces the engine's blocks exactly."""
+    docs = synth.docs_config2(1_000_000, seed=3)
+    vmin, vmax = float(docs.values.min()), float(docs.values.max())
+    lam, beta = 6000, 600
+    device_build(docs, sq_spec(vmin, vmax, lam, beta), tmp_path / "big.idx")
+    f = O.read_index_file(str(tmp_path / "big.idx"))
+    lists = f["lists"]
+    codes = O.sq_encode_u8(vmin, vmax, docs.values)
+    full = [t for t, c in enumerate(lists) if c["n_clusters"] == beta]
+    assert len(full) >= 24
+    n_trunc = 0
+    by_len = sorted(full, key=lambda t: -len(lists[t]["docs"]))
+    rest = np.random.default_rng(1).choice(by_len[12:], 12, replace=False)
+    chosen = np.array(sorted(list(by_len[:12]) + list(rest)))
+    pos = np.flatnonzero(np.isin(docs.indices, chosen))
+    rows = (np.searchsorted(docs.indptr, pos, side="right") - 1).astype(np.int32)
+    terms = docs.indices[pos]
+    L = O.ref_lib("generic")
+    P = lambda a: a.ctypes.data  # noqa: E731
+    for t in chosen:
+        m = terms == t
+        ids, vals = rows[m], codes[pos[m]]
+        # a list longer than the cap keeps its top codes in value order
+        # (inverted_lists.cpp:110-132); a shorter one keeps doc order
+        kept = ids[np.lexsort((ids, -vals.astype(np.int64)))[:lam]] if len(ids) > lam else ids
+        c = lists[t]
+        off = c["offsets"]
+        blocks = [c["docs"][off[b]:off[b + 1]] for b in range(len(off) - 1)]
+        assert sorted(np.concatenate(blocks).tolist()) == sorted(kept.tolist())
+        cents = np.array([b[0] for b in blocks], np.int32)
+        out_docs = np.empty(len(kept), np.int32)
+        out_off = np.empty(len(cents) + 1, np.int32)
+        kept = np.ascontiguousarray(kept, np.int32)
+        assert L.ref_map_docs_to_clusters(docs.dim, 1, docs.n, P(docs.indptr), P(docs.indices),
+                                          P(codes), P(kept), len(kept), P(cents), len(cents),
+                                          P(out_docs), P(out_off)) == 0
+        for b in range(len(cents)):
+            np.testing.assert_array_equal(blocks[b], out_docs[out_off[b]:out_off[b + 1]])
+        n_trunc += len(ids) > lam
+    assert n_trunc >= 4  # capped lists among those checked
+
+
 def test_sq_build_search_recall_matches_reference(tmp_path):
     docs = synth.docs_config0(20000, seed=4)
     qs = synth.queries_config0(200, seed=4)

@@ -155,7 +155,7 @@ def test_seismic_plain_equals_batched(seismic_file):
     De, Le = search_each(idx, qs, params=p2)
     np.testing.assert_array_equal(Le, Lb)
     np.testing.assert_array_equal(De, Db)
-    for wpb in (1, 2, 8):
+    for wpb in (1, 2, 8, 16, 32):
         p3 = nsparse.SeismicSearchParameters(CUT, HF)
         p3.set_engine(False, wpb)
         Dw, Lw = search(idx, qs, params=p3)
