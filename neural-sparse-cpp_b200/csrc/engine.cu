@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -145,6 +146,8 @@ __global__ void pad_rows_kernel(const int32_t* indptr, const uint16_t* idx, cons
 
 void ForwardDevice::upload(const HostCsr& h) {
     cudaStream_t s = Workspace::get().stream();
+    static std::atomic<uint64_t> uploads{0};
+    generation_ = ++uploads;
     n_docs_ = static_cast<int32_t>(h.n());
     dim_ = h.dim;
     esz_ = h.esz;
@@ -255,6 +258,8 @@ __global__ void list_meta_kernel(const int64_t* ltp, const uint16_t* sterm, int3
 
 void SeismicDevice::upload(const SeismicHost& h, int dim) {
     cudaStream_t s = Workspace::get().stream();
+    drow_.reset();
+    drow_gen_ = 0;
     n_lists_ = h.n_lists();
     words_ = (dim + 31) / 32;
     max_blocks_ = 0;
@@ -308,6 +313,33 @@ void SeismicDevice::download(SeismicHost& h) const {
     cuda_check(cudaStreamSynchronize(s), "sync");
 }
 
+namespace {
+__global__ void posting_rows_kernel(const int32_t* docs, int64_t n, const uint2* rowinfo,
+                                    int32_t n_docs, uint2* drow) {
+    for (int64_t j = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; j < n;
+         j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t d = docs[j];
+        drow[j] = (d >= 0 && d < n_docs) ? rowinfo[d] : make_uint2(0u, 0u);
+    }
+}
+}  // namespace
+
+void SeismicDevice::bind_rows(const ForwardDevice& fwd, cudaStream_t s) {
+    if (fwd.generation() == drow_gen_ && drow_.size() == docs_.size()) return;
+    const int64_t n = static_cast<int64_t>(docs_.size());
+    if (n == 0 || fwd.empty()) {
+        drow_.reset();
+        drow_gen_ = fwd.generation();
+        return;
+    }
+    if (drow_.size() != docs_.size()) drow_.resize(docs_.size());
+    posting_rows_kernel<<<device_sm_count() * 8, 256, 0, s>>>(docs_.data(), n, fwd.view().rowinfo,
+                                                              fwd.n_docs(), drow_.data());
+    cuda_check(cudaGetLastError(), "posting_rows_kernel");
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    drow_gen_ = fwd.generation();
+}
+
 SeismicView SeismicDevice::view() const {
     SeismicView v;
     v.n_lists = n_lists_;
@@ -321,12 +353,14 @@ SeismicView SeismicDevice::view() const {
     v.srun = srun_.data();
     v.sblk = sblk_.data();
     v.sval = sval_.data();
+    v.drow = (drow_.size() == docs_.size() && drow_.size() > 0) ? drow_.data() : nullptr;
     return v;
 }
 
 size_t SeismicDevice::device_bytes() const {
     return (lbp_.size() + bdp_.size() + ltp_.size() + srun_.size()) * 8 + docs_.size() * 4 +
-           lmeta_.size() * 8 + sblk_.size() * 2 + sterm_.size() * 2 + sval_.size();
+           lmeta_.size() * 8 + sblk_.size() * 2 + sterm_.size() * 2 + sval_.size() +
+           drow_.size() * 8;
 }
 
 // -------------------------------------------------------------- queries --

@@ -64,6 +64,10 @@ public:
         if (n > 0)
             cuda_check(cudaMemcpyAsync(h, p_, n * sizeof(T), cudaMemcpyDeviceToHost, s), "D2H");
     }
+    // Capacity for at least n elements, contents not kept; never shrinks.
+    void grow(size_t n) {
+        if (n_ < n) resize(n + n / 8);
+    }
     T* data() { return p_; }
     const T* data() const { return p_; }
     size_t size() const { return n_; }
@@ -122,8 +126,11 @@ public:
     int32_t n_docs() const { return n_docs_; }
     int esz() const { return esz_; }
     size_t device_bytes() const;
+    // Changes with every upload (row offsets move).
+    uint64_t generation() const { return generation_; }
 
 private:
+    uint64_t generation_ = 0;
     int32_t n_docs_ = 0;
     int dim_ = 0;
     int esz_ = 4;
@@ -155,6 +162,11 @@ public:
     bool empty() const { return n_lists_ == 0; }
     int32_t max_blocks() const { return max_blocks_; }
     size_t device_bytes() const;
+    // Copies each posting's forward-row info {start/16, length} next to its
+    // doc id (drow), so a block's candidates are read contiguously instead of
+    // through one random row-info load each; redone when `fwd` was
+    // re-uploaded since.
+    void bind_rows(const ForwardDevice& fwd, cudaStream_t s);
 
 private:
     friend struct SeismicBuilder;
@@ -168,6 +180,8 @@ private:
     DevArray<uint2> lmeta_;
     DevArray<uint16_t> sblk_;
     DevArray<uint8_t> sval_;
+    DevArray<uint2> drow_;
+    uint64_t drow_gen_ = 0;  // generation of the forward index drow_ reflects
 };
 
 // A host query batch in canonical form (terms ascending and unique per row;

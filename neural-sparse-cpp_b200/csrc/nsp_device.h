@@ -51,6 +51,7 @@ struct SeismicView {
     const int64_t* lbp;     // [n_lists + 1]
     const int64_t* bdp;     // [n_blocks + 1]
     const int32_t* docs;    // [n_list_docs]
+    const uint2* drow;      // [n_list_docs] forward rowinfo of each posting, or nullptr
     const uint2* lmeta;     // [n_lists * words]
     const int64_t* ltp;     // [n_lists + 1], column base per list
     const int64_t* srun;    // [n_columns + 1]

@@ -684,12 +684,15 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                                     hi = mid - 1;
                             }
                             const Seg& g = segs[lo];
-                            const int32_t d = __ldg(a.ix.docs + g.d0 + (i - g.cand0));
+                            const int64_t pj = g.d0 + (i - g.cand0);
+                            const int32_t d = __ldg(a.ix.docs + pj);
+                            // row info stored with the posting, else looked up
+                            uint2 ri = a.ix.drow != nullptr ? __ldg(a.ix.drow + pj)
+                                                            : __ldg(a.fwd.rowinfo + d);
                             bool member = true;
                             if (sel != nullptr)
                                 member = (__ldg(sel + (d >> 6)) >> (d & 63)) & 1ull;
-                            uint2 ri = make_uint2(0u, 0u);
-                            if (member) ri = __ldg(a.fwd.rowinfo + d);
+                            if (!member) ri = make_uint2(0u, 0u);
                             cdoc[i] = member ? d : -1;
                             coff[i] = ri.x;
                             clen[i] = ri.y;

@@ -437,7 +437,8 @@ __global__ void cut_kernel(const uint64_t* pkey_sorted, const int64_t* pair_off,
 
 template <class K, class V>
 void segmented_sort_pairs(const K* kin, K* kout, const V* vin, V* vout, int64_t n,
-                          int64_t segs, const int32_t* off, cudaStream_t s, bool stable) {
+                          int64_t segs, const int32_t* off, cudaStream_t s, bool stable,
+                          DevArray<uint8_t>* pool = nullptr) {
     if (n == 0 || segs == 0) return;
     if (n > INT32_MAX || segs > INT32_MAX) throw std::invalid_argument("build batch too large");
     size_t tmp = 0;
@@ -449,7 +450,9 @@ void segmented_sort_pairs(const K* kin, K* kout, const V* vin, V* vout, int64_t 
         cuda_check(cub::DeviceSegmentedSort::SortPairs(nullptr, tmp, kin, kout, vin, vout,
                                                        static_cast<int>(n), static_cast<int>(segs),
                                                        off, off + 1, s), "cub sort");
-    DevArray<uint8_t> t(tmp + 16);
+    DevArray<uint8_t> own;
+    DevArray<uint8_t>& t = pool != nullptr ? *pool : own;
+    t.grow(tmp + 16);
     if (stable)
         cuda_check(cub::DeviceSegmentedSort::StableSortPairs(t.data(), tmp, kin, kout, vin, vout,
                                                              static_cast<int>(n), static_cast<int>(segs),
@@ -458,23 +461,25 @@ void segmented_sort_pairs(const K* kin, K* kout, const V* vin, V* vout, int64_t 
         cuda_check(cub::DeviceSegmentedSort::SortPairs(t.data(), tmp, kin, kout, vin, vout,
                                                        static_cast<int>(n), static_cast<int>(segs),
                                                        off, off + 1, s), "cub sort");
-    cuda_check(cudaStreamSynchronize(s), "sort sync");
+    if (pool == nullptr) cuda_check(cudaStreamSynchronize(s), "sort sync");
 }
 
 template <class K>
 void segmented_sort_keys(const K* kin, K* kout, int64_t n, int64_t segs, const int32_t* off,
-                         cudaStream_t s) {
+                         cudaStream_t s, DevArray<uint8_t>* pool = nullptr) {
     if (n == 0 || segs == 0) return;
     if (n > INT32_MAX || segs > INT32_MAX) throw std::invalid_argument("build batch too large");
     size_t tmp = 0;
     cuda_check(cub::DeviceSegmentedSort::SortKeys(nullptr, tmp, kin, kout, static_cast<int>(n),
                                                   static_cast<int>(segs), off, off + 1, s),
                "cub sort");
-    DevArray<uint8_t> t(tmp + 16);
+    DevArray<uint8_t> own;
+    DevArray<uint8_t>& t = pool != nullptr ? *pool : own;
+    t.grow(tmp + 16);
     cuda_check(cub::DeviceSegmentedSort::SortKeys(t.data(), tmp, kin, kout, static_cast<int>(n),
                                                   static_cast<int>(segs), off, off + 1, s),
                "cub sort");
-    cuda_check(cudaStreamSynchronize(s), "sort sync");
+    if (pool == nullptr) cuda_check(cudaStreamSynchronize(s), "sort sync");
 }
 
 template <class T>
@@ -637,94 +642,114 @@ struct StepTimes {
 };
 thread_local StepTimes g_steps;
 
+// Device buffers of the summary pipeline, kept across batches of lists (they
+// only grow), so a batch allocates and frees nothing.
+struct SumPool {
+    DevArray<int64_t> doc_eoff, flag, pos, first_run, pair_off, kept_off, rflag, rpos, o_start,
+        o_lcol;
+    DevArray<uint16_t> ekey, skey, block_local, o_blk, o_term;
+    DevArray<uint32_t> eidx, sidx, tkey, tkey2;
+    DevArray<float> eval, delta, mass, tval, tval2;
+    DevArray<int32_t> boff, entry_block, run_start, pblock, pair_off32, keep, list_koff;
+    DevArray<uint8_t> has_delta, o_val, sort_tmp;
+    DevArray<uint64_t> pkey, pkey2;
+};
+
 template <int ESZ>
 void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
                      const DevArray<int64_t>& d_bdp, nsp::SeismicHost& L, int32_t t0, int32_t t1,
                      const std::vector<int64_t>& doc_eoff, const std::vector<int64_t>& blk_e,
-                     float alpha, cudaStream_t s) {
+                     float alpha, cudaStream_t s, SumPool& P) {
     const int sms = nsp::device_sm_count();
     const int64_t b0 = L.lbp[t0], b1 = L.lbp[t1];
     const int64_t nb = b1 - b0;
     const int64_t e0 = blk_e[b0], ne = blk_e[b1] - e0;
     // entries in block order
-    std::vector<int64_t> bdoc_eoff(doc_eoff.begin() + L.bdp[b0], doc_eoff.begin() + L.bdp[b1] + 1);
-    DevArray<int64_t> d_doc_eoff;
-    to_dev(d_doc_eoff, bdoc_eoff, s);
-    DevArray<uint16_t> ekey(ne), skey(ne);
-    DevArray<uint32_t> eidx(ne), sidx(ne);
-    DevArray<float> eval(ne);
+    const int64_t* ed = doc_eoff.data() + L.bdp[b0];
+    P.doc_eoff.upload(ed, static_cast<size_t>(L.bdp[b1] - L.bdp[b0] + 1), s);
+    P.ekey.grow(ne);
+    P.skey.grow(ne);
+    P.eidx.grow(ne);
+    P.sidx.grow(ne);
+    P.eval.grow(ne);
     entries_kernel<ESZ><<<sms * 8, 256, 0, s>>>(f, d_docs.data(), d_bdp.data(), b0, nb,
-                                                d_doc_eoff.data(), e0, ekey.data(), eidx.data(),
-                                                eval.data());
+                                                P.doc_eoff.data(), e0, P.ekey.data(),
+                                                P.eidx.data(), P.eval.data());
     cuda_check(cudaGetLastError(), "entries_kernel");
     g_steps.mark("entries");
     std::vector<int64_t> boff64(blk_e.begin() + b0, blk_e.begin() + b1 + 1);
     for (auto& v : boff64) v -= e0;
-    DevArray<int32_t> d_boff;
-    to_dev(d_boff, to_i32_offsets(boff64), s);
+    const std::vector<int32_t> boff32 = to_i32_offsets(boff64);
+    P.boff.upload(boff32.data(), boff32.size(), s);
     // stable: entries of a term stay in block order
-    segmented_sort_pairs(ekey.data(), skey.data(), eidx.data(), sidx.data(), ne, nb,
-                         d_boff.data(), s, /*stable=*/true);
-    ekey.reset();
-    eidx.reset();
+    segmented_sort_pairs(P.ekey.data(), P.skey.data(), P.eidx.data(), P.sidx.data(), ne, nb,
+                         P.boff.data(), s, /*stable=*/true, &P.sort_tmp);
     g_steps.mark("sort entries");
-    DevArray<int32_t> entry_block(ne);
-    fill_block_kernel<<<sms * 8, 256, 0, s>>>(d_boff.data(), nb, entry_block.data());
+    P.entry_block.grow(ne);
+    fill_block_kernel<<<sms * 8, 256, 0, s>>>(P.boff.data(), nb, P.entry_block.data());
     cuda_check(cudaGetLastError(), "fill_block_kernel");
-    DevArray<int64_t> flag(ne), pos(ne);
-    run_flag_kernel<<<sms * 8, 256, 0, s>>>(skey.data(), entry_block.data(), ne, flag.data());
+    P.flag.grow(ne);
+    P.pos.grow(ne);
+    run_flag_kernel<<<sms * 8, 256, 0, s>>>(P.skey.data(), P.entry_block.data(), ne,
+                                            P.flag.data());
     cuda_check(cudaGetLastError(), "run_flag_kernel");
-    nsp::exclusive_scan_i64(flag.data(), pos.data(), ne, s);
+    nsp::exclusive_scan_i64(P.flag.data(), P.pos.data(), ne, s);
     int64_t last_pos = 0, last_flag = 0;
-    cuda_check(cudaMemcpyAsync(&last_pos, pos.data() + ne - 1, 8, cudaMemcpyDeviceToHost, s), "D2H");
-    cuda_check(cudaMemcpyAsync(&last_flag, flag.data() + ne - 1, 8, cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaMemcpyAsync(&last_pos, P.pos.data() + ne - 1, 8, cudaMemcpyDeviceToHost, s),
+               "D2H");
+    cuda_check(cudaMemcpyAsync(&last_flag, P.flag.data() + ne - 1, 8, cudaMemcpyDeviceToHost, s),
+               "D2H");
     cuda_check(cudaStreamSynchronize(s), "sync");
     const int64_t n_runs = last_pos + last_flag;
     g_steps.mark("runs scan");
-    DevArray<int32_t> run_start(n_runs);
-    run_compact_kernel<<<sms * 8, 256, 0, s>>>(flag.data(), pos.data(), ne, run_start.data());
+    const int64_t nr1 = std::max<int64_t>(n_runs, 1);
+    P.run_start.grow(nr1);
+    run_compact_kernel<<<sms * 8, 256, 0, s>>>(P.flag.data(), P.pos.data(), ne,
+                                               P.run_start.data());
     cuda_check(cudaGetLastError(), "run_compact_kernel");
     // pairs per block: the run index at each block's first entry
     std::vector<int64_t> pair_off(static_cast<size_t>(nb) + 1);
     {
-        DevArray<int64_t> first_run(nb);
-        block_first_run_kernel<<<sms * 4, 256, 0, s>>>(pos.data(), d_boff.data(), nb, ne, n_runs,
-                                                       first_run.data());
+        P.first_run.grow(nb);
+        block_first_run_kernel<<<sms * 4, 256, 0, s>>>(P.pos.data(), P.boff.data(), nb, ne,
+                                                       n_runs, P.first_run.data());
         cuda_check(cudaGetLastError(), "block_first_run_kernel");
-        const std::vector<int64_t> h_first = to_host(first_run, static_cast<size_t>(nb), s);
-        for (int64_t b = 0; b < nb; ++b) pair_off[b] = h_first[b];
+        P.first_run.download(pair_off.data(), static_cast<size_t>(nb), s);
+        cuda_check(cudaStreamSynchronize(s), "D2H");
         pair_off[nb] = n_runs;
         // an empty block has no runs: its offset is the next block's
         for (int64_t b = nb - 1; b >= 0; --b)
             if (boff64[b] == boff64[b + 1]) pair_off[b] = pair_off[b + 1];
     }
-    flag.reset();
-    pos.reset();
-    DevArray<float> delta(ne);
-    DevArray<uint8_t> has_delta(ne);
-    DevArray<uint64_t> pkey(std::max<int64_t>(n_runs, 1)), pkey2(std::max<int64_t>(n_runs, 1));
-    DevArray<int32_t> pblock(std::max<int64_t>(n_runs, 1));
-    runs_kernel<ESZ><<<sms * 8, 256, 0, s>>>(skey.data(), sidx.data(), eval.data(), run_start.data(),
-                                             n_runs, ne, entry_block.data(), delta.data(),
-                                             has_delta.data(), pkey.data(), pblock.data());
+    P.delta.grow(ne);
+    P.has_delta.grow(ne);
+    P.pkey.grow(nr1);
+    P.pkey2.grow(nr1);
+    P.pblock.grow(nr1);
+    runs_kernel<ESZ><<<sms * 8, 256, 0, s>>>(P.skey.data(), P.sidx.data(), P.eval.data(),
+                                             P.run_start.data(), n_runs, ne,
+                                             P.entry_block.data(), P.delta.data(),
+                                             P.has_delta.data(), P.pkey.data(), P.pblock.data());
     cuda_check(cudaGetLastError(), "runs_kernel");
-    DevArray<float> mass(nb);
-    mass_kernel<<<sms * 4, 128, 0, s>>>(delta.data(), has_delta.data(), d_boff.data(), nb,
-                                        mass.data());
+    P.mass.grow(nb);
+    mass_kernel<<<sms * 4, 128, 0, s>>>(P.delta.data(), P.has_delta.data(), P.boff.data(), nb,
+                                        P.mass.data());
     cuda_check(cudaGetLastError(), "mass_kernel");
     g_steps.mark("runs, mass");
     // alpha cut over each block's maxima, value descending
-    DevArray<int32_t> d_pair_off32;
-    to_dev(d_pair_off32, to_i32_offsets(pair_off), s);
-    segmented_sort_keys(pkey.data(), pkey2.data(), n_runs, nb, d_pair_off32.data(), s);
-    DevArray<int64_t> d_pair_off;
-    to_dev(d_pair_off, pair_off, s);
+    const std::vector<int32_t> pair_off32 = to_i32_offsets(pair_off);
+    P.pair_off32.upload(pair_off32.data(), pair_off32.size(), s);
+    segmented_sort_keys(P.pkey.data(), P.pkey2.data(), n_runs, nb, P.pair_off32.data(), s,
+                        &P.sort_tmp);
+    P.pair_off.upload(pair_off.data(), pair_off.size(), s);
     g_steps.mark("sort maxima");
-    DevArray<int32_t> keep(nb);
-    cut_kernel<<<sms * 4, 128, 0, s>>>(pkey2.data(), d_pair_off.data(), nb, mass.data(), alpha,
-                                       keep.data());
+    P.keep.grow(nb);
+    cut_kernel<<<sms * 4, 128, 0, s>>>(P.pkey2.data(), P.pair_off.data(), nb, P.mass.data(),
+                                       alpha, P.keep.data());
     cuda_check(cudaGetLastError(), "cut_kernel");
-    const std::vector<int32_t> h_keep = to_host(keep, static_cast<size_t>(nb), s);
+    std::vector<int32_t> h_keep(static_cast<size_t>(nb));
+    P.keep.download(h_keep.data(), h_keep.size(), s);
+    cuda_check(cudaStreamSynchronize(s), "D2H");
     std::vector<int64_t> kept_off(static_cast<size_t>(nb) + 1, 0);
     for (int64_t b = 0; b < nb; ++b) kept_off[b + 1] = kept_off[b] + h_keep[b];
     const int64_t n_kept = kept_off[nb];
@@ -735,62 +760,73 @@ void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
             block_local[b - b0] = static_cast<uint16_t>(b - L.lbp[t]);
         list_koff[t - t0 + 1] = kept_off[L.lbp[t + 1] - b0];
     }
-    DevArray<int64_t> d_kept_off;
-    to_dev(d_kept_off, kept_off, s);
-    DevArray<uint16_t> d_block_local;
-    to_dev(d_block_local, block_local, s);
-    DevArray<uint32_t> tkey(std::max<int64_t>(n_kept, 1)), tkey2(std::max<int64_t>(n_kept, 1));
-    DevArray<float> tval(std::max<int64_t>(n_kept, 1)), tval2(std::max<int64_t>(n_kept, 1));
-    kept_pairs_kernel<<<sms * 8, 128, 0, s>>>(pkey2.data(), d_pair_off.data(), keep.data(),
-                                              d_kept_off.data(), d_block_local.data(), nb,
-                                              tkey.data(), tval.data());
+    P.kept_off.upload(kept_off.data(), kept_off.size(), s);
+    P.block_local.upload(block_local.data(), block_local.size(), s);
+    const int64_t nk1 = std::max<int64_t>(n_kept, 1);
+    P.tkey.grow(nk1);
+    P.tkey2.grow(nk1);
+    P.tval.grow(nk1);
+    P.tval2.grow(nk1);
+    kept_pairs_kernel<<<sms * 8, 128, 0, s>>>(P.pkey2.data(), P.pair_off.data(), P.keep.data(),
+                                              P.kept_off.data(), P.block_local.data(), nb,
+                                              P.tkey.data(), P.tval.data());
     cuda_check(cudaGetLastError(), "kept_pairs_kernel");
     g_steps.mark("alpha cut");
     // term-major per list (build_transpose, inverted_list_clusters.cpp:230-293)
-    DevArray<int32_t> d_list_koff;
-    to_dev(d_list_koff, to_i32_offsets(list_koff), s);
-    segmented_sort_pairs(tkey.data(), tkey2.data(), tval.data(), tval2.data(), n_kept, t1 - t0,
-                         d_list_koff.data(), s, /*stable=*/false);
+    const std::vector<int32_t> list_koff32 = to_i32_offsets(list_koff);
+    P.list_koff.upload(list_koff32.data(), list_koff32.size(), s);
+    segmented_sort_pairs(P.tkey.data(), P.tkey2.data(), P.tval.data(), P.tval2.data(), n_kept,
+                         t1 - t0, P.list_koff.data(), s, /*stable=*/false, &P.sort_tmp);
     g_steps.mark("transpose sort");
     // columns assembled on the device: block ids, values, and one run per
     // (list, term) with its start
     const int32_t nl = t1 - t0;
-    DevArray<uint16_t> o_blk(std::max<int64_t>(n_kept, 1));
-    DevArray<uint8_t> o_val(std::max<int64_t>(n_kept, 1) * ESZ);
-    DevArray<int64_t> rflag(static_cast<size_t>(n_kept) + 1), rpos(static_cast<size_t>(n_kept) + 1);
-    columns_kernel<ESZ><<<sms * 8, 256, 0, s>>>(tkey2.data(), tval2.data(), n_kept, o_blk.data(),
-                                                o_val.data(), rflag.data());
+    P.o_blk.grow(nk1);
+    P.o_val.grow(nk1 * ESZ);
+    P.rflag.grow(n_kept + 1);
+    P.rpos.grow(n_kept + 1);
+    columns_kernel<ESZ><<<sms * 8, 256, 0, s>>>(P.tkey2.data(), P.tval2.data(), n_kept,
+                                                P.o_blk.data(), P.o_val.data(), P.rflag.data());
     cuda_check(cudaGetLastError(), "columns_kernel");
-    list_start_kernel<<<std::max(1, (nl + 255) / 256), 256, 0, s>>>(d_list_koff.data(), nl,
-                                                                    n_kept, rflag.data());
+    list_start_kernel<<<std::max(1, (nl + 255) / 256), 256, 0, s>>>(P.list_koff.data(), nl,
+                                                                    n_kept, P.rflag.data());
     cuda_check(cudaGetLastError(), "list_start_kernel");
-    nsp::exclusive_scan_i64(rflag.data(), rpos.data(), n_kept + 1, s);
+    nsp::exclusive_scan_i64(P.rflag.data(), P.rpos.data(), n_kept + 1, s);
     int64_t n_cols = 0;
-    cuda_check(cudaMemcpyAsync(&n_cols, rpos.data() + n_kept, 8, cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaMemcpyAsync(&n_cols, P.rpos.data() + n_kept, 8, cudaMemcpyDeviceToHost, s),
+               "D2H");
     cuda_check(cudaStreamSynchronize(s), "sync");
-    DevArray<uint16_t> o_term(std::max<int64_t>(n_cols, 1));
-    DevArray<int64_t> o_start(std::max<int64_t>(n_cols, 1)), o_lcol(static_cast<size_t>(nl) + 1);
-    column_compact_kernel<<<sms * 8, 256, 0, s>>>(tkey2.data(), rflag.data(), rpos.data(), n_kept,
-                                                  o_term.data(), o_start.data());
+    P.o_term.grow(std::max<int64_t>(n_cols, 1));
+    P.o_start.grow(std::max<int64_t>(n_cols, 1));
+    P.o_lcol.grow(static_cast<size_t>(nl) + 1);
+    column_compact_kernel<<<sms * 8, 256, 0, s>>>(P.tkey2.data(), P.rflag.data(), P.rpos.data(),
+                                                  n_kept, P.o_term.data(), P.o_start.data());
     cuda_check(cudaGetLastError(), "column_compact_kernel");
-    list_cols_kernel<<<std::max(1, (nl + 1 + 255) / 256), 256, 0, s>>>(d_list_koff.data(), nl,
-                                                                       rpos.data(), o_lcol.data());
+    list_cols_kernel<<<std::max(1, (nl + 1 + 255) / 256), 256, 0, s>>>(
+        P.list_koff.data(), nl, P.rpos.data(), P.o_lcol.data());
     cuda_check(cudaGetLastError(), "list_cols_kernel");
-    const std::vector<uint16_t> h_blk = to_host(o_blk, static_cast<size_t>(n_kept), s);
-    const std::vector<uint8_t> h_val = to_host(o_val, static_cast<size_t>(n_kept) * ESZ, s);
-    const std::vector<uint16_t> h_term = to_host(o_term, static_cast<size_t>(n_cols), s);
-    const std::vector<int64_t> h_start = to_host(o_start, static_cast<size_t>(n_cols), s);
-    const std::vector<int64_t> h_lcol = to_host(o_lcol, static_cast<size_t>(nl) + 1, s);
+    // straight into the host arrays' tails
+    const size_t eb = L.sblk.size(), vb = L.sval.size(), cb = L.sterm.size();
+    L.sblk.resize(eb + static_cast<size_t>(n_kept));
+    L.sval.resize(vb + static_cast<size_t>(n_kept) * ESZ);
+    L.sterm.resize(cb + static_cast<size_t>(n_cols));
+    std::vector<int64_t> h_start(static_cast<size_t>(n_cols));
+    std::vector<int64_t> h_lcol(static_cast<size_t>(nl) + 1);
+    P.o_blk.download(L.sblk.data() + eb, static_cast<size_t>(n_kept), s);
+    P.o_val.download(L.sval.data() + vb, static_cast<size_t>(n_kept) * ESZ, s);
+    P.o_term.download(L.sterm.data() + cb, static_cast<size_t>(n_cols), s);
+    P.o_start.download(h_start.data(), h_start.size(), s);
+    P.o_lcol.download(h_lcol.data(), h_lcol.size(), s);
+    cuda_check(cudaStreamSynchronize(s), "D2H");
     g_steps.mark("columns, D2H");
-    const int64_t ebase = static_cast<int64_t>(L.sblk.size());
-    const int64_t cbase = static_cast<int64_t>(L.sterm.size());
-    L.sblk.insert(L.sblk.end(), h_blk.begin(), h_blk.end());
-    L.sval.insert(L.sval.end(), h_val.begin(), h_val.end());
-    L.sterm.insert(L.sterm.end(), h_term.begin(), h_term.end());
+    const int64_t ebase = static_cast<int64_t>(eb);
+    const int64_t cbase = static_cast<int64_t>(cb);
     // srun holds column boundaries: the first column starts where the last
     // batch ended (srun.back() == ebase)
-    for (int64_t c = 1; c < n_cols; ++c) L.srun.push_back(ebase + h_start[c]);
-    if (n_cols > 0) L.srun.push_back(ebase + n_kept);
+    const size_t rb = L.srun.size();
+    L.srun.resize(rb + static_cast<size_t>(std::max<int64_t>(n_cols, 0)));
+    for (int64_t c = 1; c < n_cols; ++c) L.srun[rb + c - 1] = ebase + h_start[c];
+    if (n_cols > 0) L.srun[rb + n_cols - 1] = ebase + n_kept;
     for (int32_t l = 0; l < nl; ++l) L.ltp.push_back(cbase + h_lcol[l + 1]);
     g_steps.mark("host append");
 }
@@ -996,6 +1032,7 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
     to_dev(d_docs, L.docs, s);
     const int64_t budget = int64_t{1} << 27;  // entries per batch
     g_steps.start(s);
+    SumPool pool;
     L.ltp.assign(1, 0);
     L.srun.assign(1, 0);
     L.sterm.clear();
@@ -1013,7 +1050,7 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
             t0 = t1;
             continue;
         }
-        summarize_batch<ESZ>(f, d_docs, d_bdp, L, t0, t1, doc_eoff, blk_e, p.alpha, s);
+        summarize_batch<ESZ>(f, d_docs, d_bdp, L, t0, t1, doc_eoff, blk_e, p.alpha, s, pool);
         t0 = t1;
     }
 

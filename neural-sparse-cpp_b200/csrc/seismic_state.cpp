@@ -12,6 +12,7 @@ void SeismicState::ensure_lists() {
         lists_dev.upload(lists, vectors.host.dim);
         dev_valid = true;
     }
+    if (dev_valid) lists_dev.bind_rows(vectors.dev, nsp::Workspace::get().stream());
 }
 
 const nsp::SeismicHost& SeismicState::host_lists() {
