@@ -134,6 +134,22 @@ def recall_at_k(L, T):
     return float(np.mean(v)) if v else 1.0
 
 
+def replica_throughput(total_ms, e2e_s, n_queries, steps, e2e_steps, world, device=None):
+    """Whole-job throughput of `world` replicas, each searching its own
+    `n_queries` per step: every rank's time is replaced by the slowest rank's
+    (max over ranks), so the job rate is world * queries / that time. Returns
+    (max timed ms, queries/s, e2e queries/s); identical on every rank."""
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t_ = torch.tensor([float(total_ms), float(e2e_s)], dtype=torch.float64, device=device)
+        dist.all_reduce(t_, op=dist.ReduceOp.MAX)
+        total_ms, e2e_s = float(t_[0].item()), float(t_[1].item())
+    value = world * n_queries * steps / (total_ms / 1000.0)
+    e2e_value = world * n_queries * e2e_steps / e2e_s
+    return total_ms, value, e2e_value
+
+
 def cpu_baseline(docs, qs, index_file, sample):
     """The reference's own search (compiled from its sources, oracle/_ref), all
     host threads, on the first `sample` queries of the workload."""
@@ -312,17 +328,8 @@ def run_engine(args):
     del brute
 
     # ---- aggregate over ranks: max time
-    my_ms = total_ms
-    if world > 1:
-        t_ = torch.tensor([my_ms], device=dev)
-        torch.distributed.all_reduce(t_, op=torch.distributed.ReduceOp.MAX)
-        my_ms = float(t_.item())
-    value = world * qs.n * args.steps / (my_ms / 1000.0)
-    e2e_value = world * qs.n * len(e2e_t) / sum(e2e_t)
-    if world > 1:
-        t_ = torch.tensor([sum(e2e_t)], device=dev)
-        torch.distributed.all_reduce(t_, op=torch.distributed.ReduceOp.MAX)
-        e2e_value = world * qs.n * len(e2e_t) / float(t_.item())
+    my_ms, value, e2e_value = replica_throughput(total_ms, sum(e2e_t), qs.n, args.steps,
+                                                 len(e2e_t), world, dev)
 
     peak, peak_kind = measured_peaks()
     achieved = st.bytes / (st.kernel_ms / 1000.0) / 1e9
