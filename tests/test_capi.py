@@ -151,6 +151,30 @@ def test_search_params():
     assert q.vmax == 2.0
 
 
+def test_kernel_and_engine_knobs_are_validated():
+    p = nsparse.SeismicSearchParameters(10, 1.0)
+    for variant, tuning in ((-1, 0), (0, 0), (1, 4096), (2, 256), (5, 8192)):
+        p.set_kernel(variant, tuning)
+    for variant, tuning in ((-2, 0), (6, 0), (2, 8193), (1, 1 << 20), (3, -1)):
+        with pytest.raises(ValueError):
+            p.set_kernel(variant, tuning)
+    p.set_engine(False, 32)
+    with pytest.raises(ValueError):
+        p.set_engine(False, 33)
+
+
+def test_autotune_and_server_need_a_seismic_index():
+    idx = nsparse.index_factory(64, "brutal")
+    ip, ix, v = small_csr()
+    idx.add(5, ip, ix, v)
+    with pytest.raises(ValueError, match="seismic"):
+        idx.autotune(5, ip, ix, v, 3)
+    with pytest.raises(ValueError, match="seismic"):
+        nsparse.Server(idx)
+    with pytest.raises(ValueError, match="must not be negative"):
+        nsparse.Server(nsparse.index_factory(64, "seismic"), max_batch=-1)
+
+
 def test_quantizer_range_is_validated():
     with pytest.raises(ValueError, match="vmax must be greater than vmin"):
         nsparse.index_factory(64, "seismic_sq,quantizer=8bit|vmin=1|vmax=1")
