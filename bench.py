@@ -247,6 +247,12 @@ def run_engine(args):
     log(f"rank {rank}: device build {build_s:.1f}s")
     params = nsparse.SeismicSearchParameters(CUT, HF)
     params.set_kernel(args.variant, args.tuning)
+    tuned = None
+    if args.variant < 0:
+        # the engine's autotuner picks the launch shape on a 2,000-query sample
+        sample = qs.rows(0, min(qs.n, 2000))
+        tuned = idx.autotune(sample.n, sample.indptr, sample.indices, sample.values, K, params)
+        log(f"autotune: {tuned}")
 
     # ---- device-resident inputs and outputs
     d_ip = torch.from_numpy(qs.indptr).to(dev)
@@ -354,7 +360,7 @@ def run_engine(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": dict(WORKLOAD, parallelism=f"replicas{world}",
                                                 kernel_variant=args.variant,
-                                                kernel_tuning=args.tuning),
+                                                kernel_tuning=args.tuning, autotuned=tuned),
             "recall_at_10": rec, "build_s": build_s,
             "plain": {"qps": plain_qps, "queries": n_plain,
                       "p50_ms": lat_ms[len(lat_ms) // 2], "p99_ms": lat_ms[int(0.99 * (len(lat_ms) - 1))],
@@ -465,6 +471,13 @@ def run_engine_sq(args):
     stream = torch.cuda.Stream()
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     peak, peak_kind = measured_peaks()
+    tp = nsparse.SeismicSearchParameters(12, 0.9)
+    tp.set_kernel(args.variant, args.tuning)
+    tuned = None
+    if args.variant < 0:
+        sample = qs.rows(0, 4096)
+        tuned = idx.autotune(sample.n, sample.indptr, sample.indices, sample.values, K, tp)
+        log(f"autotune: {tuned}")
     sweep = []
     for cut, hf in SQ_SWEEP:
         params = nsparse.SeismicSearchParameters(cut, hf)
@@ -543,7 +556,8 @@ def run_engine_sq(args):
                       "cut": head["cut"], "k": K, "heap_factor": head["heap_factor"],
                       "l2": "flushed between passes; index > L2",
                       "kernel_variant": args.variant, "kernel_tuning": args.tuning},
-           "build_s": build_s, "sweep": sweep, "serving": serving, "peak_gbs": peak,
+           "build_s": build_s, "autotuned": tuned, "sweep": sweep, "serving": serving,
+           "peak_gbs": peak,
            "peak_source": peak_kind}
     print(json.dumps(out))
 
