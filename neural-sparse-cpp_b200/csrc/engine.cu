@@ -283,6 +283,37 @@ void SeismicDevice::upload(const SeismicHost& h, int dim) {
     cuda_check(cudaStreamSynchronize(s), "sync");
 }
 
+void SeismicDevice::adopt(const std::vector<int64_t>& lbp, const std::vector<int64_t>& bdp,
+                          const std::vector<int64_t>& ltp, int esz, int dim,
+                          DevArray<int32_t>&& docs, DevArray<uint16_t>&& sterm,
+                          DevArray<int64_t>&& srun, DevArray<uint16_t>&& sblk,
+                          DevArray<uint8_t>&& sval) {
+    cudaStream_t s = Workspace::get().stream();
+    drow_.reset();
+    drow_gen_ = 0;
+    n_lists_ = static_cast<int32_t>(lbp.size()) - 1;
+    words_ = (dim + 31) / 32;
+    max_blocks_ = 0;
+    for (int32_t t = 0; t < n_lists_; ++t)
+        max_blocks_ = std::max<int32_t>(max_blocks_, static_cast<int32_t>(lbp[t + 1] - lbp[t]));
+    esz_ = esz;
+    lbp_.upload(lbp.data(), lbp.size(), s);
+    bdp_.upload(bdp.data(), bdp.size(), s);
+    ltp_.upload(ltp.data(), ltp.size(), s);
+    docs_ = std::move(docs);
+    sterm_ = std::move(sterm);
+    srun_ = std::move(srun);
+    sblk_ = std::move(sblk);
+    sval_ = std::move(sval);
+    if (n_lists_ > 0) {
+        lmeta_.resize(static_cast<size_t>(n_lists_) * words_);
+        list_meta_kernel<<<std::min(n_lists_, 148 * 8), 256, static_cast<size_t>(words_) * 4, s>>>(
+            ltp_.data(), sterm_.data(), n_lists_, words_, lmeta_.data());
+        cuda_check(cudaGetLastError(), "list_meta_kernel");
+    }
+    cuda_check(cudaStreamSynchronize(s), "sync");
+}
+
 void SeismicDevice::download(SeismicHost& h) const {
     cudaStream_t s = Workspace::get().stream();
     h.esz = esz_;

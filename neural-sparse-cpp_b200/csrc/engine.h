@@ -157,6 +157,13 @@ struct SeismicHost {
 class SeismicDevice {
 public:
     void upload(const SeismicHost& h, int dim);
+    // Takes lists built on the device: the offset arrays come from the host,
+    // the per-posting and per-entry arrays are moved in (their capacity may
+    // exceed what the offsets use).
+    void adopt(const std::vector<int64_t>& lbp, const std::vector<int64_t>& bdp,
+               const std::vector<int64_t>& ltp, int esz, int dim, DevArray<int32_t>&& docs,
+               DevArray<uint16_t>&& sterm, DevArray<int64_t>&& srun, DevArray<uint16_t>&& sblk,
+               DevArray<uint8_t>&& sval);
     void download(SeismicHost& h) const;
     SeismicView view() const;
     bool empty() const { return n_lists_ == 0; }

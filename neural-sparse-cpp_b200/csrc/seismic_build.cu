@@ -642,6 +642,46 @@ struct StepTimes {
 };
 thread_local StepTimes g_steps;
 
+// Summary columns of all lists built so far, in device memory: the index's
+// final arrays, handed to the device image without a round trip through
+// host memory (the host copy is made only if it is asked for, e.g. to write
+// the index file).
+struct DevColumns {
+    DevArray<uint16_t> sterm, sblk;
+    DevArray<int64_t> srun;
+    DevArray<uint8_t> sval;
+    size_t n_cols = 0;     // sterm used; srun holds n_cols + 1 boundaries
+    size_t n_entries = 0;  // sblk used; sval holds n_entries * esz bytes
+};
+
+// Appends n elements at src (device) after the first `used` of dst, growing
+// dst geometrically.
+template <class T>
+void dev_append(DevArray<T>& dst, size_t used, const T* src, size_t n, cudaStream_t s) {
+    if (used + n > dst.size()) {
+        DevArray<T> bigger(std::max(dst.size() * 2, used + n));
+        if (used > 0)
+            cuda_check(cudaMemcpyAsync(bigger.data(), dst.data(), used * sizeof(T),
+                                       cudaMemcpyDeviceToDevice, s),
+                       "D2D");
+        cuda_check(cudaStreamSynchronize(s), "sync");
+        dst = std::move(bigger);
+    }
+    if (n > 0)
+        cuda_check(cudaMemcpyAsync(dst.data() + used, src, n * sizeof(T), cudaMemcpyDeviceToDevice,
+                                   s),
+                   "D2D");
+}
+
+// Column boundaries of a batch: column c > 0 starts where column c-1 ends;
+// the last ends after the batch's n_kept entries; all offset by `ebase`.
+__global__ void column_bounds_kernel(const int64_t* start, int64_t n_cols, int64_t ebase,
+                                     int64_t n_kept, int64_t* srun_tail) {
+    for (int64_t c = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; c < n_cols;
+         c += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        srun_tail[c] = ebase + (c + 1 < n_cols ? start[c + 1] : n_kept);
+}
+
 // Device buffers of the summary pipeline, kept across batches of lists (they
 // only grow), so a batch allocates and frees nothing.
 struct SumPool {
@@ -659,7 +699,7 @@ template <int ESZ>
 void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
                      const DevArray<int64_t>& d_bdp, nsp::SeismicHost& L, int32_t t0, int32_t t1,
                      const std::vector<int64_t>& doc_eoff, const std::vector<int64_t>& blk_e,
-                     float alpha, cudaStream_t s, SumPool& P) {
+                     float alpha, cudaStream_t s, SumPool& P, DevColumns& out) {
     const int sms = nsp::device_sm_count();
     const int64_t b0 = L.lbp[t0], b1 = L.lbp[t1];
     const int64_t nb = b1 - b0;
@@ -805,30 +845,33 @@ void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
     list_cols_kernel<<<std::max(1, (nl + 1 + 255) / 256), 256, 0, s>>>(
         P.list_koff.data(), nl, P.rpos.data(), P.o_lcol.data());
     cuda_check(cudaGetLastError(), "list_cols_kernel");
-    // straight into the host arrays' tails
-    const size_t eb = L.sblk.size(), vb = L.sval.size(), cb = L.sterm.size();
-    L.sblk.resize(eb + static_cast<size_t>(n_kept));
-    L.sval.resize(vb + static_cast<size_t>(n_kept) * ESZ);
-    L.sterm.resize(cb + static_cast<size_t>(n_cols));
-    std::vector<int64_t> h_start(static_cast<size_t>(n_cols));
+    // appended to the index's device columns; only the per-list column
+    // counts come back to the host
+    const size_t eb = out.n_entries, cb = out.n_cols;
+    dev_append(out.sblk, eb, P.o_blk.data(), static_cast<size_t>(n_kept), s);
+    dev_append(out.sval, eb * ESZ, P.o_val.data(), static_cast<size_t>(n_kept) * ESZ, s);
+    dev_append(out.sterm, cb, P.o_term.data(), static_cast<size_t>(n_cols), s);
+    if (out.srun.size() < cb + 1 + static_cast<size_t>(n_cols)) {
+        DevArray<int64_t> bigger(
+            std::max(out.srun.size() * 2, cb + 1 + static_cast<size_t>(n_cols)));
+        cuda_check(cudaMemcpyAsync(bigger.data(), out.srun.data(), (cb + 1) * sizeof(int64_t),
+                                   cudaMemcpyDeviceToDevice, s),
+                   "D2D");
+        cuda_check(cudaStreamSynchronize(s), "sync");
+        out.srun = std::move(bigger);
+    }
+    if (n_cols > 0)
+        column_bounds_kernel<<<sms * 4, 256, 0, s>>>(P.o_start.data(), n_cols,
+                                                     static_cast<int64_t>(eb), n_kept,
+                                                     out.srun.data() + cb + 1);
+    cuda_check(cudaGetLastError(), "column_bounds_kernel");
     std::vector<int64_t> h_lcol(static_cast<size_t>(nl) + 1);
-    P.o_blk.download(L.sblk.data() + eb, static_cast<size_t>(n_kept), s);
-    P.o_val.download(L.sval.data() + vb, static_cast<size_t>(n_kept) * ESZ, s);
-    P.o_term.download(L.sterm.data() + cb, static_cast<size_t>(n_cols), s);
-    P.o_start.download(h_start.data(), h_start.size(), s);
     P.o_lcol.download(h_lcol.data(), h_lcol.size(), s);
     cuda_check(cudaStreamSynchronize(s), "D2H");
-    g_steps.mark("columns, D2H");
-    const int64_t ebase = static_cast<int64_t>(eb);
-    const int64_t cbase = static_cast<int64_t>(cb);
-    // srun holds column boundaries: the first column starts where the last
-    // batch ended (srun.back() == ebase)
-    const size_t rb = L.srun.size();
-    L.srun.resize(rb + static_cast<size_t>(std::max<int64_t>(n_cols, 0)));
-    for (int64_t c = 1; c < n_cols; ++c) L.srun[rb + c - 1] = ebase + h_start[c];
-    if (n_cols > 0) L.srun[rb + n_cols - 1] = ebase + n_kept;
-    for (int32_t l = 0; l < nl; ++l) L.ltp.push_back(cbase + h_lcol[l + 1]);
-    g_steps.mark("host append");
+    out.n_entries += static_cast<size_t>(n_kept);
+    out.n_cols += static_cast<size_t>(n_cols);
+    for (int32_t l = 0; l < nl; ++l) L.ltp.push_back(static_cast<int64_t>(cb) + h_lcol[l + 1]);
+    g_steps.mark("columns");
 }
 
 // Phase timings on stderr when NSP_VERBOSE=1 (the engine's one debug switch).
@@ -1038,6 +1081,9 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
     L.sterm.clear();
     L.sblk.clear();
     L.sval.clear();
+    DevColumns cols;
+    cols.srun.resize(1);
+    cuda_check(cudaMemsetAsync(cols.srun.data(), 0, sizeof(int64_t), s), "memset");
     int32_t t0 = 0;
     while (t0 < n_lists) {
         int32_t t1 = t0 + 1;
@@ -1050,18 +1096,23 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
             t0 = t1;
             continue;
         }
-        summarize_batch<ESZ>(f, d_docs, d_bdp, L, t0, t1, doc_eoff, blk_e, p.alpha, s, pool);
+        summarize_batch<ESZ>(f, d_docs, d_bdp, L, t0, t1, doc_eoff, blk_e, p.alpha, s, pool,
+                             cols);
         t0 = t1;
     }
 
     clock.mark("summaries");
     g_steps.print();
-    // ---- 6. publish
+    // ---- 6. publish: the device image takes the built arrays; the host copy
+    // is filled on demand (host_lists)
     std::lock_guard<std::mutex> g(st.mu);
-    st.lists = std::move(L);
+    st.lists_dev.adopt(L.lbp, L.bdp, L.ltp, ESZ, dim, std::move(d_docs), std::move(cols.sterm),
+                       std::move(cols.srun), std::move(cols.sblk), std::move(cols.sval));
+    st.lists = nsp::SeismicHost{};
+    st.lists.esz = ESZ;
     st.list_esz.assign(static_cast<size_t>(n_lists), static_cast<uint8_t>(ESZ));
-    st.host_valid = true;
-    st.dev_valid = false;
+    st.host_valid = false;
+    st.dev_valid = true;
 }
 
 }  // namespace
