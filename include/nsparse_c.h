@@ -197,6 +197,51 @@ nsp_status_t nsp_index_autotune(nsp_index_t* index, int32_t n, const int32_t* in
                                 const nsp_search_params_t* params, int* variant, int* batch_docs,
                                 int* warps_per_block, float* kernel_ms);
 
+/* ---- CUDA-graph search steps (extension with no counterpart in the
+ * reference; each step returns what nsp_index_search_device returns for the
+ * same rows) -------------------------------------------------------------
+ *
+ * A batched SEISMIC search step of `n` query rows, captured once as a CUDA
+ * graph and replayed per batch: the counter resets, the query encode of a
+ * quantized index and the persistent search kernel become one graph launch,
+ * with the kernel's scratch owned by the graph (no allocation per step).
+ * Parameters (k, cut, heap factor, kernel, an id selector's doc set) are
+ * fixed at capture; `nnz_cap` bounds the query entries of a step and
+ * `max_row_nnz` one row's. The index must stay alive and unchanged: after an
+ * add, build or read the step is refused (NSP_ERR_RUNTIME); capture anew.
+ * IDMapIndex and selectors with at most k ids (the exact-match path) are
+ * rejected. One step of a graph is in flight at a time. */
+typedef struct nsp_search_graph nsp_search_graph_t;
+/* Device buffers of a step: n+1 row offsets, nnz_cap terms and values
+ * (rows canonical: terms ascending and unique), n*k results. */
+typedef struct {
+    int32_t* indptr;
+    uint16_t* indices;
+    float* values;
+    float* distances;
+    int32_t* labels;
+} nsp_graph_buffers_t;
+/* `device_buffers`: the caller's buffers (kept alive by the caller), or NULL
+ * for buffers the graph allocates (all rows empty until written). */
+nsp_status_t nsp_search_graph_new(nsp_index_t* index, int32_t n, int32_t nnz_cap,
+                                  int32_t max_row_nnz, int k, const nsp_search_params_t* params,
+                                  const nsp_graph_buffers_t* device_buffers,
+                                  nsp_search_graph_t** out);
+nsp_status_t nsp_search_graph_free(nsp_search_graph_t* graph);
+nsp_status_t nsp_search_graph_buffers(const nsp_search_graph_t* graph, nsp_graph_buffers_t* out);
+/* Replays the step on `cuda_stream` (NULL = the graph's own stream), after
+ * the work queued there (e.g. the copies that wrote the rows); returns. */
+nsp_status_t nsp_search_graph_launch(nsp_search_graph_t* graph, void* cuda_stream);
+/* Waits for `cuda_stream` (NULL = the graph's own stream); reports a kernel
+ * error of the step and makes its counters the thread's last search stats. */
+nsp_status_t nsp_search_graph_sync(nsp_search_graph_t* graph, void* cuda_stream);
+/* Host rows in, host results out (n <= the graph's rows; rows in any order
+ * of terms, as nsp_index_search takes them): copies through pinned staging,
+ * one graph launch, waits. */
+nsp_status_t nsp_search_graph_search(nsp_search_graph_t* graph, int32_t n, const int32_t* indptr,
+                                     const uint16_t* indices, const float* values,
+                                     float* distances, int32_t* labels);
+
 /* ---- serving loop (extension with no counterpart in the reference) ------
  * Single-query requests, each with its own k and an optional doc filter, are
  * batched continuously: `slots` worker threads (one CUDA stream each) take

@@ -304,6 +304,71 @@ nsp_status_t nsp_index_autotune(nsp_index_t* index, int32_t n, const int32_t* in
     });
 }
 
+struct nsp_search_graph {
+    std::unique_ptr<nsparse::detail::IndexSearchGraph> g;
+};
+
+nsp_status_t nsp_search_graph_new(nsp_index_t* index, int32_t n, int32_t nnz_cap,
+                                  int32_t max_row_nnz, int k, const nsp_search_params_t* params,
+                                  const nsp_graph_buffers_t* device_buffers,
+                                  nsp_search_graph_t** out) {
+    return guarded([&] {
+        if (index == nullptr || out == nullptr) throw std::invalid_argument("unexpected nullptr");
+        nsp::GraphBuffers b;
+        if (device_buffers != nullptr) {
+            b.indptr = device_buffers->indptr;
+            b.indices = device_buffers->indices;
+            b.values = device_buffers->values;
+            b.distances = device_buffers->distances;
+            b.labels = device_buffers->labels;
+        }
+        auto h = std::make_unique<nsp_search_graph>();
+        h->g = std::make_unique<detail::IndexSearchGraph>(as_index(index), n, nnz_cap,
+                                                          max_row_nnz, k, as_params(params),
+                                                          device_buffers != nullptr ? &b : nullptr);
+        *out = h.release();
+    });
+}
+
+nsp_status_t nsp_search_graph_free(nsp_search_graph_t* graph) {
+    return guarded([&] { delete graph; });
+}
+
+nsp_status_t nsp_search_graph_buffers(const nsp_search_graph_t* graph, nsp_graph_buffers_t* out) {
+    return guarded([&] {
+        if (graph == nullptr || out == nullptr) throw std::invalid_argument("unexpected nullptr");
+        const nsp::GraphBuffers& b = graph->g->buffers();
+        out->indptr = b.indptr;
+        out->indices = b.indices;
+        out->values = b.values;
+        out->distances = b.distances;
+        out->labels = b.labels;
+    });
+}
+
+nsp_status_t nsp_search_graph_launch(nsp_search_graph_t* graph, void* cuda_stream) {
+    return guarded([&] {
+        if (graph == nullptr) throw std::invalid_argument("unexpected nullptr");
+        graph->g->launch(static_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
+nsp_status_t nsp_search_graph_sync(nsp_search_graph_t* graph, void* cuda_stream) {
+    return guarded([&] {
+        if (graph == nullptr) throw std::invalid_argument("unexpected nullptr");
+        graph->g->sync(static_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
+nsp_status_t nsp_search_graph_search(nsp_search_graph_t* graph, int32_t n, const int32_t* indptr,
+                                     const uint16_t* indices, const float* values,
+                                     float* distances, int32_t* labels) {
+    return guarded([&] {
+        if (graph == nullptr) throw std::invalid_argument("unexpected nullptr");
+        graph->g->search(n, indptr, indices, values, distances, labels);
+    });
+}
+
 struct nsp_server {
     std::unique_ptr<nsparse::detail::Server> s;
 };

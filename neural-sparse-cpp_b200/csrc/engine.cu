@@ -65,7 +65,7 @@ Workspace& Workspace::get() {
     return *ws;
 }
 
-void* Workspace::dev(Slot s, size_t bytes) {
+void* Workspace::dev(int s, size_t bytes) {
     if (bytes == 0) bytes = 16;
     if (dcap_[s] < bytes) {
         cuda_check(cudaStreamSynchronize(stream_), "workspace sync");
@@ -256,8 +256,13 @@ __global__ void list_meta_kernel(const int64_t* ltp, const uint16_t* sterm, int3
 
 }  // namespace
 
+namespace {
+std::atomic<uint64_t> g_list_generation{0};
+}  // namespace
+
 void SeismicDevice::upload(const SeismicHost& h, int dim) {
     cudaStream_t s = Workspace::get().stream();
+    generation_ = ++g_list_generation;
     drow_.reset();
     drow_gen_ = 0;
     n_lists_ = h.n_lists();
@@ -289,6 +294,7 @@ void SeismicDevice::adopt(const std::vector<int64_t>& lbp, const std::vector<int
                           DevArray<int64_t>&& srun, DevArray<uint16_t>&& sblk,
                           DevArray<uint8_t>&& sval) {
     cudaStream_t s = Workspace::get().stream();
+    generation_ = ++g_list_generation;
     drow_.reset();
     drow_gen_ = 0;
     n_lists_ = static_cast<int32_t>(lbp.size()) - 1;
@@ -357,6 +363,7 @@ __global__ void posting_rows_kernel(const int32_t* docs, int64_t n, const uint2*
 
 void SeismicDevice::bind_rows(const ForwardDevice& fwd, cudaStream_t s) {
     if (fwd.generation() == drow_gen_ && drow_.size() == docs_.size()) return;
+    generation_ = ++g_list_generation;
     const int64_t n = static_cast<int64_t>(docs_.size());
     if (n == 0 || fwd.empty()) {
         drow_.reset();
@@ -587,10 +594,12 @@ SeismicPlan plan_seismic(int kind, int words, int qcap, int k, int n_queries,
 // (variant 4) measured fastest at 1M docs (2.9x variant 0).
 constexpr int kDefaultVariant = 4;
 
+}  // namespace
+
 void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
                  const int32_t* d_indptr, const uint16_t* d_idx, const void* d_vals, int32_t qcap,
                  const SeismicSearchArgs& args_in, const uint64_t* d_sel, float* d_out,
-                 int32_t* d_lab, cudaStream_t s, Workspace& ws, SearchStats* stats) {
+                 int32_t* d_lab, cudaStream_t s, Scratch& ws, SearchStats* stats) {
     SeismicSearchArgs args = args_in;
     if (args.variant < 0) args.variant = kDefaultVariant;
     if (args.d_sel_q != nullptr && args.variant < 2)
@@ -620,9 +629,17 @@ void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
         ws.dev(Workspace::kStats, kStatCount * sizeof(unsigned long long)));
     cuda_check(cudaMemsetAsync(st, 0, kStatCount * sizeof(unsigned long long), s), "memset");
     a.stats = st;
-    cudaEvent_t e0, e1;
-    cuda_check(cudaEventCreate(&e0), "event");
-    cuda_check(cudaEventCreate(&e1), "event");
+    // The kernel's own time, only when asked for: an event recorded inside a
+    // stream capture would outlive this call in the graph.
+    const bool timed = stats != nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (timed) {
+        cuda_check(cudaEventCreate(&e0), "event");
+        cuda_check(cudaEventCreate(&e1), "event");
+    }
+    auto mark = [&](cudaEvent_t e) {
+        if (timed) cuda_check(cudaEventRecord(e, s), "event");
+    };
     int launches = 0;
     auto* err = static_cast<int32_t*>(ws.dev(Workspace::kErr, sizeof(int32_t)));
     cuda_check(cudaMemsetAsync(err, 0, sizeof(int32_t), s), "memset");
@@ -653,20 +670,20 @@ void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
             a.work_counter = static_cast<int32_t*>(ws.dev(Workspace::kCounter, sizeof(int32_t)));
             cuda_check(cudaMemsetAsync(a.work_counter, 0, sizeof(int32_t), s), "memset");
             a.first_query = 0;
-            cuda_check(cudaEventRecord(e0, s), "event");
+            mark(e0);
             cuda_check(launch_seismic_cta(kind, a, p.wpb, p.blocks, s), "seismic search launch");
-            cuda_check(cudaEventRecord(e1, s), "event");
+            mark(e1);
             launches = 1;
         } else {
             // one launch per query, one CTA
             a.work_counter = nullptr;
-            cuda_check(cudaEventRecord(e0, s), "event");
+            mark(e0);
             for (int32_t q = 0; q < n; ++q) {
                 a.first_query = q;
                 a.q.n = q + 1;
                 cuda_check(launch_seismic_cta(kind, a, p.wpb, 1, s), "seismic search launch");
             }
-            cuda_check(cudaEventRecord(e1, s), "event");
+            mark(e1);
             launches = n;
         }
     } else if (!args.plain) {
@@ -680,9 +697,9 @@ void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
         a.work_counter = static_cast<int32_t*>(ws.dev(Workspace::kCounter, sizeof(int32_t)));
         cuda_check(cudaMemsetAsync(a.work_counter, 0, sizeof(int32_t), s), "memset");
         a.first_query = 0;
-        cuda_check(cudaEventRecord(e0, s), "event");
+        mark(e0);
         cuda_check(launch_seismic(kind, a, p.wpb, p.blocks, s), "seismic search launch");
-        cuda_check(cudaEventRecord(e1, s), "event");
+        mark(e1);
         launches = 1;
     } else {
         // One launch per query: a single warp walks the query (the per-query
@@ -695,13 +712,13 @@ void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
         a.bcap = p.bcap;
         a.bscore = static_cast<float*>(ws.dev(Workspace::kBScore, a.ix.max_blocks * sizeof(float)));
         a.work_counter = nullptr;
-        cuda_check(cudaEventRecord(e0, s), "event");
+        mark(e0);
         for (int32_t q = 0; q < n; ++q) {
             a.first_query = q;
             a.q.n = q + 1;
             cuda_check(launch_seismic(kind, a, 1, 1, s), "seismic search launch");
         }
-        cuda_check(cudaEventRecord(e1, s), "event");
+        mark(e1);
         launches = n;
     }
     if (stats != nullptr) {
@@ -717,14 +734,56 @@ void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
         stats->kernel_ms = ms;
         stats->launches = launches;
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    if (timed) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
 }
+
+void reserve_seismic_scratch(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
+                             int32_t max_nnz, const SeismicSearchArgs& args_in) {
+    if (n <= 0) return;
+    SeismicSearchArgs args = args_in;
+    if (args.variant < 0) args.variant = kDefaultVariant;
+    Workspace& ws = Workspace::get();
+    const size_t nq = static_cast<size_t>(n);
+    const size_t nnz = nq * static_cast<size_t>(std::max(max_nnz, 1));
+    const size_t cnt = nq * static_cast<size_t>(args.k);
+    // the sizes upload_queries, download_results and run_seismic ask for
+    ws.pinned(Workspace::kQIndptr, (nq + 1) * sizeof(int32_t));
+    ws.pinned(Workspace::kQIdx, nnz * sizeof(uint16_t));
+    ws.pinned(Workspace::kQVal, nnz * sizeof(float));
+    ws.pinned(Workspace::kOutD, cnt * sizeof(float));
+    ws.pinned(Workspace::kOutL, cnt * sizeof(int32_t));
+    ws.dev(Workspace::kQIndptr, (nq + 1) * sizeof(int32_t));
+    ws.dev(Workspace::kQIdx, nnz * sizeof(uint16_t) + 16);
+    ws.dev(Workspace::kQVal, nnz * sizeof(float) + 16);
+    if (args.qbits != 0) ws.dev(Workspace::kQCode, nnz * 2 + 16);
+    ws.dev(Workspace::kOutD, cnt * sizeof(float));
+    ws.dev(Workspace::kOutL, cnt * sizeof(int32_t));
+    ws.dev(Workspace::kStats, kStatCount * sizeof(unsigned long long));
+    ws.dev(Workspace::kErr, sizeof(int32_t));
+    ws.dev(Workspace::kCounter, sizeof(int32_t));
+    if (args.variant < 2) return;
+    const SeismicPlan p = plan_seismic_cta(val_kind_of(args.qbits), fwd.view().dim,
+                                           std::max(max_nnz, 1), args.k, n, args, args.plain);
+    const int maxb = std::max(ix.max_blocks(), 1);
+    const size_t order_stride = static_cast<size_t>((maxb + 7) & ~7);
+    ws.dev(Workspace::kBScore, static_cast<size_t>(p.blocks) * p.wpb * maxb * sizeof(float));
+    ws.dev(Workspace::kOrder, static_cast<size_t>(p.blocks) * order_stride * sizeof(uint16_t));
+    int p2 = 1;
+    while (p2 < maxb) p2 <<= 1;
+    if (p2 > 2 * p.batch_docs)
+        ws.dev(Workspace::kSortKeys,
+               static_cast<size_t>(p.blocks) * p2 * sizeof(unsigned long long));
+}
+
+namespace {
 
 // Raises if a search kernel on `s` flagged an error (call after sync):
 // 1 a bounded wait gave up, 2 a sort buffer was missing, 3 a query longer
 // than the launch's query capacity.
-void check_kernel_error(Workspace& ws, cudaStream_t s) {
+void check_kernel_error(Scratch& ws, cudaStream_t s) {
     int32_t h = 0;
     auto* err = static_cast<int32_t*>(ws.dev(Workspace::kErr, sizeof(int32_t)));
     cuda_check(cudaMemcpyAsync(&h, err, sizeof(int32_t), cudaMemcpyDeviceToHost, s), "D2H");

@@ -77,10 +77,20 @@ private:
     size_t n_ = 0;
 };
 
+// Device scratch by slot, grow-only: the per-thread Workspace, or the
+// buffers a captured search graph owns.
+class Scratch {
+public:
+    virtual void* dev(int slot, size_t bytes) = 0;
+
+protected:
+    ~Scratch() = default;
+};
+
 // Per-thread stream plus grow-only device and pinned scratch, so concurrent
 // searches from several host threads never share buffers (the reference's
 // per-thread scratch, seismic_index.cpp:197-201).
-class Workspace {
+class Workspace : public Scratch {
 public:
     enum Slot : int {
         kQIndptr, kQIdx, kQVal, kQCode, kOutD, kOutL, kSel, kBScore, kCounter, kStats,
@@ -88,7 +98,7 @@ public:
     };
     static Workspace& get();
     cudaStream_t stream() const { return stream_; }
-    void* dev(Slot s, size_t bytes);
+    void* dev(int s, size_t bytes) override;
     void* pinned(Slot s, size_t bytes);
     ~Workspace();
 
@@ -189,6 +199,11 @@ private:
     DevArray<uint8_t> sval_;
     DevArray<uint2> drow_;
     uint64_t drow_gen_ = 0;  // generation of the forward index drow_ reflects
+    uint64_t generation_ = 0;
+
+public:
+    // Changes whenever a device array of the lists is replaced.
+    uint64_t generation() const { return generation_; }
 };
 
 // A host query batch in canonical form (terms ascending and unique per row;
@@ -255,11 +270,87 @@ void exact_search(const ForwardDevice& fwd, const QueryBatch& q, int k, int mode
 void exact_list_search(const ForwardDevice& fwd, const QueryBatch& q, const SeismicSearchArgs& args,
                        const std::vector<int32_t>& ids, float* out_d, int32_t* out_l);
 
+// Enqueues one SEISMIC search on `s`, its scratch drawn from `scratch`. With
+// `stats` null nothing on the host waits for the device (so the call can be
+// captured into a CUDA graph); else it waits and fills the kernel's time and
+// counters.
+void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
+                 const int32_t* d_indptr, const uint16_t* d_idx, const void* d_vals, int32_t qcap,
+                 const SeismicSearchArgs& args, const uint64_t* d_sel, float* d_out,
+                 int32_t* d_lab, cudaStream_t s, Scratch& scratch, SearchStats* stats);
+
+// Grows the calling thread's workspace to what seismic_search of `n`
+// queries of up to `max_nnz` terms with `args` asks for, so a later search
+// within those bounds allocates nothing (growing a buffer frees the old one,
+// and cudaFree waits for the whole device).
+void reserve_seismic_scratch(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
+                             int32_t max_nnz, const SeismicSearchArgs& args);
+
 // Device-resident variant: queries, outputs and stream owned by the caller.
 void seismic_search_device(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
                            const int32_t* d_indptr, const uint16_t* d_idx, const void* d_val,
                            int32_t max_nnz, const SeismicSearchArgs& args, const uint64_t* d_sel,
                            float* d_out, int32_t* d_lab, cudaStream_t s, SearchStats* stats);
+
+// Device buffers of a captured search step: the queries in CSR form (`n`
+// rows, room for `nnz_cap` entries; rows with terms ascending and unique) and
+// the results (n x k, row-major).
+struct GraphBuffers {
+    int32_t* indptr = nullptr;
+    uint16_t* indices = nullptr;
+    float* values = nullptr;
+    float* distances = nullptr;
+    int32_t* labels = nullptr;
+};
+
+// One batched SEISMIC search step captured once as a CUDA graph and replayed
+// for every batch: the resets of the step's counters, the query encode of a
+// quantized index and the persistent search kernel run as one graph launch on
+// buffers fixed at capture. The scratch belongs to the graph, so replays need
+// no allocation and no host synchronisation. One step of a graph is in flight
+// at a time (its launches are ordered on the stream they are given).
+class SearchGraph {
+public:
+    // `bind`: the caller's device buffers for queries and results (kept alive
+    // by the caller), or null for buffers the graph allocates. `sel_bits`: a
+    // doc bitmap every query of every step is filtered by, or null.
+    SearchGraph(const ForwardDevice& fwd, const SeismicDevice& ix, const SeismicSearchArgs& args,
+                int32_t n, int32_t nnz_cap, int32_t qcap, const std::vector<uint64_t>* sel_bits,
+                const GraphBuffers* bind);
+    ~SearchGraph();
+    SearchGraph(const SearchGraph&) = delete;
+    SearchGraph& operator=(const SearchGraph&) = delete;
+
+    const GraphBuffers& buffers() const { return buf_; }
+    int32_t n() const { return n_; }
+    int32_t nnz_cap() const { return nnz_cap_; }
+    int32_t qcap() const { return qcap_; }
+    int k() const { return args_.k; }
+    cudaStream_t stream() const { return stream_; }
+    // Replays the step on `s`, after the work already queued there.
+    void launch(cudaStream_t s);
+    // Waits for `s` and raises if the kernel flagged an error (as the
+    // ordinary search does); `stats` (optional) gets the step's counters.
+    void check(cudaStream_t s, SearchStats* stats = nullptr);
+    // Host queries in (canonical, at most n rows), host results out: staged
+    // copies and one graph launch on the graph's own stream.
+    void search_host(const QueryBatch& q, float* out_d, int32_t* out_l,
+                     SearchStats* stats = nullptr);
+
+private:
+    struct Owned;
+    void enqueue(cudaStream_t s);
+    const ForwardDevice& fwd_;
+    const SeismicDevice& ix_;
+    SeismicSearchArgs args_;
+    int32_t n_, nnz_cap_, qcap_;
+    GraphBuffers buf_;
+    std::unique_ptr<Owned> own_;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t done_ = nullptr;  // recorded after each launch
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t exec_ = nullptr;
+};
 
 }  // namespace nsp
 

@@ -349,9 +349,15 @@ const IDSelectorEnumerable* exact_match_selector(const IDSelector* sel, int k) {
 }
 
 // The autotuner's launch shape, where the caller left the choice to the engine.
-void apply_tuned(const SeismicState& st, nsp::SeismicSearchArgs& a) {
+// The tuned variant applies to every launch. The tuned batch and warps were
+// chosen among 4- and 8-warp CTAs on a large batch, so they apply only where
+// the planner itself would fill every SM with several CTAs (more than two
+// queries per SM, not the one-query plain path); smaller launches keep the
+// planner's wider CTAs, which finish a lone query sooner.
+void apply_tuned(const SeismicState& st, nsp::SeismicSearchArgs& a, int64_t n_queries) {
     if (a.variant >= 0 || st.tuned.variant < 0) return;
     a.variant = st.tuned.variant;
+    if (a.plain || n_queries <= 2 * static_cast<int64_t>(nsp::device_sm_count())) return;
     if (a.batch_docs == 0) a.batch_docs = st.tuned.batch_docs;
     if (a.warps_per_block == 0) a.warps_per_block = st.tuned.warps_per_block;
 }
@@ -360,7 +366,7 @@ void seismic_search_common(SeismicState& st, int dim, idx_t n, const idx_t* indp
                            const term_t* indices, const float* values, int k, float* distances,
                            idx_t* labels, SearchParameters* params, nsp::SeismicSearchArgs args) {
     if (st.vectors.host.n() == 0) return fill_padding(n, k, distances, labels);
-    apply_tuned(st, args);
+    apply_tuned(st, args, n);
     st.vectors.ensure_device();
     const nsp::QueryBatch q = nsp::canonicalize(n, indptr, indices, values, dim);
     const IDSelector* sel = params == nullptr ? nullptr : params->get_id_selector();
@@ -553,7 +559,7 @@ void search_device(Index* index, int32_t n, const int32_t* d_indptr, const uint1
     }
     if (st->vectors.host.n() == 0) throw std::runtime_error("index is empty");
     if (max_nnz < 0) throw std::invalid_argument("max_row_nnz must not be negative");
-    apply_tuned(*st, a);
+    apply_tuned(*st, a, n);
     const IDSelector* sel = params == nullptr ? nullptr : params->get_id_selector();
     if (exact_match_selector(sel, k) != nullptr)
         throw std::invalid_argument("device-resident search does not take the exact-match path");
@@ -583,6 +589,61 @@ void search_device(Index* index, int32_t n, const int32_t* d_indptr, const uint1
     }
     nsp::seismic_search_device(st->vectors.dev, st->lists_dev, n, d_indptr, d_idx, vals, max_nnz,
                                a, d_sel, d_out, d_lab, s, nullptr);
+}
+
+IndexSearchGraph::IndexSearchGraph(Index* index, int32_t n, int32_t nnz_cap, int32_t max_nnz,
+                                   int k, SearchParameters* params,
+                                   const nsp::GraphBuffers* bind) {
+    throw_if_not_positive(n);
+    throw_if_not_positive(k);
+    if (nnz_cap < 0 || max_nnz < 0) throw std::invalid_argument("nnz must not be negative");
+    if (dynamic_cast<IDMapIndex*>(index) != nullptr)
+        throw std::invalid_argument("a search graph runs on a seismic index, not an IDMapIndex");
+    nsp::SeismicSearchArgs a;
+    st_ = resolve_seismic(index, params, k, a);
+    dim_ = index->get_dimension();
+    if (st_->vectors.host.n() == 0) throw std::runtime_error("index is empty");
+    apply_tuned(*st_, a, n);
+    const IDSelector* sel = params == nullptr ? nullptr : params->get_id_selector();
+    if (exact_match_selector(sel, k) != nullptr)
+        throw std::invalid_argument("a search graph does not take the exact-match path");
+    st_->vectors.ensure_device();
+    st_->ensure_lists();
+    std::vector<uint64_t> bits;
+    if (sel != nullptr) bits = selector_bitmap(sel, st_->vectors.host.n());
+    fwd_gen_ = st_->vectors.dev.generation();
+    ix_gen_ = st_->lists_dev.generation();
+    g_ = std::make_unique<nsp::SearchGraph>(st_->vectors.dev, st_->lists_dev, a, n, nnz_cap,
+                                            max_nnz, sel != nullptr ? &bits : nullptr, bind);
+}
+
+void IndexSearchGraph::ensure_current() const {
+    if (st_->vectors.dirty || st_->vectors.dev.generation() != fwd_gen_ ||
+        st_->lists_dev.generation() != ix_gen_)
+        throw std::runtime_error(
+            "the index changed since the search graph was captured; capture a new one");
+}
+
+void IndexSearchGraph::launch(cudaStream_t s) {
+    ensure_current();
+    g_->launch(s == nullptr ? g_->stream() : s);
+}
+
+void IndexSearchGraph::sync(cudaStream_t s) {
+    nsp::SearchStats st;
+    g_->check(s == nullptr ? g_->stream() : s, &st);
+    record_stats(st);
+}
+
+void IndexSearchGraph::search(idx_t n, const idx_t* indptr, const term_t* indices,
+                              const float* values, float* distances, idx_t* labels) {
+    throw_if_not_positive(n);
+    throw_if_any_null(indptr, indices, values, distances, labels);
+    ensure_current();
+    const nsp::QueryBatch q = nsp::canonicalize(n, indptr, indices, values, dim_);
+    nsp::SearchStats st;
+    g_->search_host(q, distances, labels, &st);
+    record_stats(st);
 }
 
 SeismicState* resolve_seismic(Index* index, SearchParameters* params, int k,

@@ -5,6 +5,7 @@
 #define NSP_INDEX_STATE_H
 
 #include <cstdint>
+#include <memory>
 #include <mutex>
 #include <vector>
 
@@ -58,7 +59,7 @@ SeismicState* resolve_seismic(Index* index, SearchParameters* params, int k,
                               nsp::SeismicSearchArgs& a);
 
 // The autotuner's launch shape, where the caller left the choice to the engine.
-void apply_tuned(const SeismicState& st, nsp::SeismicSearchArgs& a);
+void apply_tuned(const SeismicState& st, nsp::SeismicSearchArgs& a, int64_t n_queries);
 
 // Times every one-CTA-per-query launch shape (lanes per doc x batch x warps)
 // on a sample of queries and keeps the fastest for later searches that leave
@@ -72,6 +73,32 @@ nsp::KernelChoice seismic_autotune(Index* index, idx_t n, const idx_t* indptr,
 void search_device(Index* index, int32_t n, const int32_t* d_indptr, const uint16_t* d_idx,
                    const float* d_val, int32_t max_nnz, int k, float* d_out, int32_t* d_lab,
                    SearchParameters* params, cudaStream_t s);
+
+// One batched search step of a seismic index captured as a CUDA graph
+// (nsparse_c.h, nsp_search_graph_*). It refuses to run once the index's
+// device arrays were replaced (add, build, read) since the capture.
+class IndexSearchGraph {
+public:
+    IndexSearchGraph(Index* index, int32_t n, int32_t nnz_cap, int32_t max_nnz, int k,
+                     SearchParameters* params, const nsp::GraphBuffers* bind);
+    const nsp::GraphBuffers& buffers() const { return g_->buffers(); }
+    nsp::SearchGraph& graph() { return *g_; }
+    // Replays the step on `s` (null: the graph's own stream) and returns.
+    void launch(cudaStream_t s);
+    // Waits for `s` (null: the graph's own stream), raises a kernel error,
+    // records the step's counters as the thread's last search stats.
+    void sync(cudaStream_t s);
+    // Host queries in, host results out (at most the graph's rows).
+    void search(idx_t n, const idx_t* indptr, const term_t* indices, const float* values,
+                float* distances, idx_t* labels);
+
+private:
+    void ensure_current() const;
+    SeismicState* st_ = nullptr;
+    int dim_ = 0;
+    uint64_t fwd_gen_ = 0, ix_gen_ = 0;
+    std::unique_ptr<nsp::SearchGraph> g_;
+};
 
 }  // namespace detail
 }  // namespace nsparse

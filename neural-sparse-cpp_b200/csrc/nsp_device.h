@@ -131,7 +131,8 @@ struct ExactLaunch {
     unsigned long long* stats;
 };
 
-// Lets kernel `f` use the device's whole opt-in shared memory. Every call sets
+// Lets kernel `f` use the device's whole opt-in shared memory (less its own
+// static shared memory, which counts against the same limit). Every call sets
 // the same value, so launches from several host threads cannot undo one
 // another's setting, as a per-launch size could between a set and a launch.
 template <class F>
@@ -142,7 +143,11 @@ inline cudaError_t allow_opt_in_smem(F f) {
     int v = 0;
     e = cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    cudaFuncAttributes fa{};
+    e = cudaFuncGetAttributes(&fa, f);
+    if (e != cudaSuccess) return e;
+    const int dyn = v - static_cast<int>(fa.sharedSizeBytes);
+    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn > 0 ? dyn : 0);
 }
 
 // Launchers (return cudaError_t of the launch). `sm_count` sizes persistent

@@ -180,6 +180,41 @@ __device__ __forceinline__ int partial(const uint16_t* ip, const uint8_t* vp, in
     return acc;
 }
 
+// Two consecutive steps of uint8 codes (elements at ip and ip + stride,
+// `rem` and `rem2` of them real): both steps' loads are issued before either
+// is used, so a row of up to two steps costs one memory round trip.
+template <typename TE>
+__device__ __forceinline__ int partial2(const uint16_t* ip, const uint8_t* vp, int rem, int rem2,
+                                        int stride, const TE* tbl) {
+    if (rem <= 0) return 0;
+    uint32_t t[8], t2[8];
+    uint4 v, v2 = make_uint4(0u, 0u, 0u, 0u);
+    ldg256(ip, t);
+    v = __ldg(reinterpret_cast<const uint4*>(vp));
+    if (rem2 > 0) {
+        ldg256(ip + stride, t2);
+        v2 = __ldg(reinterpret_cast<const uint4*>(vp + stride));
+    }
+    int acc = 0;
+    {
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            const int q = static_cast<int>(tbl[term_of(t, u)]);
+            acc += static_cast<int>((w[u >> 2] >> (8 * (u & 3))) & 0xffu) * q;
+        }
+    }
+    if (rem2 > 0) {
+        const uint32_t w[4] = {v2.x, v2.y, v2.z, v2.w};
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            const int q = static_cast<int>(tbl[term_of(t2, u)]);
+            acc += static_cast<int>((w[u >> 2] >> (8 * (u & 3))) & 0xffu) * q;
+        }
+    }
+    return acc;
+}
+
 // uint16 codes: int64 sum (distance.h:49-57).
 template <typename TE>
 __device__ __forceinline__ long long partial(const uint16_t* ip, const uint16_t* vp, int rem,
@@ -237,14 +272,17 @@ __device__ __forceinline__ float finish(long long a) { return static_cast<float>
 // group claims one candidate of the batch at a time and walks its row kG*16
 // elements per step, lane l of the group taking elements 16l..16l+15 of the
 // step, so a step's loads are kG*32 contiguous bytes of ids and the matching
-// contiguous values. A group whose row ends takes the next candidate at the
-// following step.
+// contiguous values (uint8 rows: two steps per iteration). A group whose row
+// ends takes the next candidate at the following iteration.
 template <typename V, typename TE, bool kMask, int kG>
 __device__ void score_batch(const FwdView& fwd, Ctl* ctl, const TE* tbl, const float* qv,
                             const uint32_t* coff, const uint32_t* clen, float* csc, int total,
                             int lane) {
     using A = typename Acc<V>::T;
     constexpr bool kF32 = std::is_same<V, float>::value;
+    // uint8 rows advance two steps per iteration (partial2)
+    constexpr bool kU8Steps2 = std::is_same<V, uint8_t>::value;
+    constexpr int kStep = (kU8Steps2 ? 32 : 16) * kG;
     const uint16_t* idx_base = fwd.idx;
     const V* val_base = static_cast<const V*>(fwd.val);
     const int gl = lane & (kG - 1);
@@ -284,13 +322,15 @@ __device__ void score_batch(const FwdView& fwd, Ctl* ctl, const TE* tbl, const f
             float p[16];
             products<TE, kMask>(ip, vp, mine, tbl, qv, p);
             acc = fold<kG>(acc, p, gbase);
+        } else if constexpr (kU8Steps2) {
+            acc += group_sum<kG>(partial2<TE>(ip, vp, mine, mine - 16 * kG, 16 * kG, tbl));
         } else {
             acc += group_sum<kG>(partial<TE>(ip, vp, mine, tbl));
         }
         if (act) {
-            ip += 16 * kG;
-            vp += 16 * kG;
-            rem -= 16 * kG;
+            ip += kStep;
+            vp += kStep;
+            rem -= kStep;
             if (rem <= 0) {
                 if (gl == 0) csc[i] = finish(acc);
                 i = -1;

@@ -197,6 +197,7 @@ struct AssignArgs {
     int64_t max_centroid_entries;
     int64_t max_kept;
     int32_t max_nc;
+    int32_t sims_in_smem;  // 1: the similarity rows are in dynamic shared memory
 };
 
 template <int ESZ>
@@ -216,8 +217,12 @@ __global__ void __launch_bounds__(256) assign_kernel(AssignArgs a) {
     uint16_t* ccl = a.ccl + static_cast<size_t>(blockIdx.x) * a.max_centroid_entries;
     uint8_t* cw = a.cw + static_cast<size_t>(blockIdx.x) * a.max_centroid_entries * ESZ;
     uint8_t* isc = a.is_centroid + static_cast<size_t>(blockIdx.x) * a.max_kept;
-    acc_t* sims = static_cast<acc_t*>(a.sims) +
-                  static_cast<size_t>(blockIdx.x * wpb + warp) * a.max_nc;
+    // each warp's row of similarities: shared memory when the launch gave
+    // room for it (the read-modify-writes of one doc are serial), else global
+    extern __shared__ __align__(16) unsigned char dyn[];
+    acc_t* sims = a.sims_in_smem ? reinterpret_cast<acc_t*>(dyn) + static_cast<size_t>(warp) * a.max_nc
+                                 : static_cast<acc_t*>(a.sims) +
+                                       static_cast<size_t>(blockIdx.x * wpb + warp) * a.max_nc;
     const uint8_t* fval = static_cast<const uint8_t*>(a.f.val);
 
     for (;;) {
@@ -1023,7 +1028,15 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
         a.max_centroid_entries = max_ce;
         a.max_kept = std::max<int64_t>(max_kept, 1);
         a.max_nc = std::max(max_nc, 1);
-        assign_kernel<ESZ><<<ctas, wpb * 32, 0, s>>>(a);
+        const size_t acc_bytes = ESZ == 4 ? 4 : 8;
+        const size_t sims_smem = static_cast<size_t>(wpb) * a.max_nc * acc_bytes;
+        size_t smem = 0;
+        if (sims_smem <= 96u * 1024u) {
+            cuda_check(nsp::allow_opt_in_smem(assign_kernel<ESZ>), "assign smem");
+            a.sims_in_smem = 1;
+            smem = sims_smem;
+        }
+        assign_kernel<ESZ><<<ctas, wpb * 32, smem, s>>>(a);
         cuda_check(cudaGetLastError(), "assign_kernel");
         cuda_check(cudaStreamSynchronize(s), "assign sync");
     }

@@ -29,6 +29,11 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+// Bounds the workers reserve scratch for up front (larger requests still run;
+// their batches grow the scratch once).
+constexpr int kReserveK = 100;
+constexpr int kReserveNnz = 256;
+
 int64_t request_bytes(const ServerRequest& r) {
     // query terms and values, results, one selector pointer
     return static_cast<int64_t>(r.terms.size()) * 6 + 4 + static_cast<int64_t>(r.k) * 8 + 8;
@@ -171,9 +176,12 @@ void Server::replay(int32_t n, const int32_t* indptr, const uint16_t* indices, c
         enqueue(reqs[i]);
     }
     {
+        // requests finish roughly in order: the scan resumes where it stopped
+        size_t j = 0;
         std::unique_lock<std::mutex> lk(mu_);
         cv_done_.wait(lk, [&] {
-            return std::all_of(reqs.begin(), reqs.end(), [](const auto& r) { return r->done; });
+            while (j < reqs.size() && reqs[j]->done) ++j;
+            return j == reqs.size();
         });
     }
     for (int32_t i = 0; i < n; ++i) {
@@ -210,6 +218,28 @@ ServerStats Server::stats() const {
 void Server::worker() {
     if (cudaSetDevice(device_) != cudaSuccess) return;
     nsp::DevArray<const uint64_t*> d_sel;  // this worker's per-query selector table
+    try {
+        // Scratch for every batch size up to max_batch (rows up to kReserveNnz
+        // terms, k up to kReserveK) before the first request: a buffer grown
+        // mid-stream frees the old one, and that cudaFree waits for every
+        // worker's work on the device.
+        d_sel.resize(static_cast<size_t>(cfg_.max_batch));
+        const int sms = nsp::device_sm_count();
+        for (int k : {10, kReserveK}) {
+            SeismicSearchParameters params(10, 1.0f);
+            nsp::SeismicSearchArgs a;
+            resolve_seismic(index_, &params, k, a);
+            for (int n : {1, sms / 2, sms, 2 * sms, 2 * sms + 1, 4 * sms, cfg_.max_batch}) {
+                if (n < 1 || n > cfg_.max_batch) continue;
+                nsp::SeismicSearchArgs t = a;
+                apply_tuned(*st_, t, n);
+                if (t.variant >= 0 && t.variant < 2) t.variant = -1;
+                nsp::reserve_seismic_scratch(st_->vectors.dev, st_->lists_dev, n, kReserveNnz, t);
+            }
+        }
+    } catch (const std::exception&) {
+        // a failed reservation only means later batches grow their scratch
+    }
     for (;;) {
         std::vector<std::shared_ptr<ServerRequest>> batch;
         std::vector<const uint64_t*> sel;
@@ -270,7 +300,7 @@ void Server::worker() {
             SeismicSearchParameters params(batch[0]->cut, batch[0]->hf);
             nsp::SeismicSearchArgs a;
             resolve_seismic(index_, &params, k, a);
-            apply_tuned(*st_, a);
+            apply_tuned(*st_, a, static_cast<int64_t>(batch.size()));
             if (a.variant >= 0 && a.variant < 2) a.variant = -1;  // needs one CTA per query
             const bool any =
                 std::any_of(sel.begin(), sel.end(), [](const uint64_t* p) { return p != nullptr; });

@@ -488,3 +488,77 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+class _GraphBuffers(ctypes.Structure):
+    _fields_ = [("indptr", _P), ("indices", _P), ("values", _P), ("distances", _P),
+                ("labels", _P)]
+
+
+_sig("nsp_search_graph_new", _P, _I32, _I32, _I32, ctypes.c_int, _P,
+     ctypes.POINTER(_GraphBuffers), ctypes.POINTER(_P))
+_sig("nsp_search_graph_free", _P)
+_sig("nsp_search_graph_buffers", _P, ctypes.POINTER(_GraphBuffers))
+_sig("nsp_search_graph_launch", _P, _P)
+_sig("nsp_search_graph_sync", _P, _P)
+_sig("nsp_search_graph_search", _P, _I32, _P, _P, _P, _P, _P)
+
+
+class SearchGraph:
+    """Extension: one batched SEISMIC search step of `n` query rows captured
+    as a CUDA graph and replayed per batch (k, parameters and selector fixed
+    at capture). `device_buffers`: a dict of device pointers (ints) "indptr",
+    "indices", "values", "distances", "labels" the caller keeps alive, or None
+    for buffers the graph owns. Keep the index alive and unchanged while the
+    graph is used."""
+
+    def __init__(self, index, n, nnz_cap, max_row_nnz, k, params=None, device_buffers=None):
+        self._index, self._params = index, params
+        self.n, self.k = int(n), int(k)
+        b = None
+        if device_buffers is not None:
+            b = _GraphBuffers(*(device_buffers[f] for f in
+                                ("indptr", "indices", "values", "distances", "labels")))
+        h = _P()
+        _check(_L.nsp_search_graph_new(index._h, self.n, int(nnz_cap), int(max_row_nnz), self.k,
+                                       None if params is None else params._h,
+                                       None if b is None else ctypes.byref(b), ctypes.byref(h)))
+        self._h = h.value
+
+    def buffers(self):
+        b = _GraphBuffers()
+        _check(_L.nsp_search_graph_buffers(self._h, ctypes.byref(b)))
+        return {f: getattr(b, f) for f, _ in _GraphBuffers._fields_}
+
+    def launch(self, stream=None):
+        """Replays the step on `stream` (a cudaStream_t as int; None: the
+        graph's own stream) and returns."""
+        _check(_L.nsp_search_graph_launch(self._h, stream))
+
+    def sync(self, stream=None):
+        _check(_L.nsp_search_graph_sync(self._h, stream))
+
+    def search(self, n, indptr, indices, values):
+        """Host rows in (at most the graph's n), (distances, labels) out."""
+        indptr = np.ascontiguousarray(indptr, dtype=np.int32)
+        indices = np.ascontiguousarray(indices, dtype=np.uint16)
+        values = np.ascontiguousarray(values, dtype=np.float32)
+        n = int(n)
+        if n <= 0:
+            raise ValueError("value must be positive")
+        distances = np.empty((n, self.k), dtype=np.float32)
+        labels = np.empty((n, self.k), dtype=np.int32)
+        _check(_L.nsp_search_graph_search(self._h, n, _ptr(indptr), _ptr(indices), _ptr(values),
+                                          _ptr(distances), _ptr(labels)))
+        return distances, labels
+
+    def close(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            _L.nsp_search_graph_free(h)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
