@@ -28,6 +28,10 @@ struct EngineOptions {
     int variant = -1;
     int stage_bytes = 0;
     int batch_docs = 0;
+    // CTAs per query for variants 2-5: 0 lets the engine choose, 1 one CTA,
+    // 2, 4 or 8 a thread-block cluster whose CTAs score each query's batches
+    // together (lower latency per query; identical results).
+    int ctas_per_query = 0;
 };
 
 struct SearchParameters {

@@ -128,6 +128,11 @@ nsp_status_t nsp_search_params_set_engine(nsp_search_params_t* params, int plain
  * docs per batch (0 = default). Results do not depend on either. */
 nsp_status_t nsp_search_params_set_kernel(nsp_search_params_t* params, int variant,
                                           int tuning);
+/* Extension: CTAs per query of SEISMIC variants 2-5 (0 engine's choice, 1 one
+ * CTA, 2/4/8 a thread-block cluster: the CTAs score each batch of the query's
+ * candidates together, for lower latency per query). Results do not depend on
+ * it. */
+nsp_status_t nsp_search_params_set_split(nsp_search_params_t* params, int ctas_per_query);
 nsp_status_t nsp_search_params_free(nsp_search_params_t* params);
 
 /* ---- engine extensions -------------------------------------------------- */
@@ -187,15 +192,16 @@ nsp_status_t nsp_index_search_device_noalloc(nsp_index_t* index, int32_t n,
 
 /* Kernel autotuner. Times each one-CTA-per-query launch shape of the SEISMIC
  * search (lanes per doc, candidate docs per batch, warps per CTA) on the n
- * sample queries with the given parameters and keeps the fastest for this
- * index: later searches whose parameters leave the kernel to the engine
- * (variant -1) use it. Results do not depend on the choice. Writes the choice
- * to the out pointers (any may be NULL). Extension with no counterpart in the
- * reference. */
+ * sample queries with the given parameters, then the CTAs per query (1, 2, 4,
+ * 8) of one-query launches on up to 16 of them searched alone, and keeps the
+ * fastest for this index: later searches whose parameters leave the kernel to
+ * the engine (variant -1) use it. Results do not depend on the choice. Writes
+ * the choice to the out pointers (any may be NULL). Extension with no
+ * counterpart in the reference. */
 nsp_status_t nsp_index_autotune(nsp_index_t* index, int32_t n, const int32_t* indptr,
                                 const uint16_t* indices, const float* values, int k,
                                 const nsp_search_params_t* params, int* variant, int* batch_docs,
-                                int* warps_per_block, float* kernel_ms);
+                                int* warps_per_block, float* kernel_ms, int* ctas_per_query);
 
 /* ---- CUDA-graph search steps (extension with no counterpart in the
  * reference; each step returns what nsp_index_search_device returns for the

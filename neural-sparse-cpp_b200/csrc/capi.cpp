@@ -260,6 +260,16 @@ nsp_status_t nsp_search_params_set_kernel(nsp_search_params_t* params, int varia
     });
 }
 
+nsp_status_t nsp_search_params_set_split(nsp_search_params_t* params, int ctas_per_query) {
+    return guarded([&] {
+        if (params == nullptr) throw std::invalid_argument("unexpected nullptr");
+        if (ctas_per_query != 0 && ctas_per_query != 1 && ctas_per_query != 2 &&
+            ctas_per_query != 4 && ctas_per_query != 8)
+            throw std::invalid_argument("ctas_per_query must be 0, 1, 2, 4 or 8");
+        as_params(params)->engine.ctas_per_query = ctas_per_query;
+    });
+}
+
 nsp_status_t nsp_search_params_free(nsp_search_params_t* params) {
     return guarded([&] { delete as_params(params); });
 }
@@ -292,7 +302,7 @@ nsp_status_t nsp_index_search_device(nsp_index_t* index, int32_t n, const int32_
 nsp_status_t nsp_index_autotune(nsp_index_t* index, int32_t n, const int32_t* indptr,
                                 const uint16_t* indices, const float* values, int k,
                                 const nsp_search_params_t* params, int* variant, int* batch_docs,
-                                int* warps_per_block, float* kernel_ms) {
+                                int* warps_per_block, float* kernel_ms, int* ctas_per_query) {
     return guarded([&] {
         if (index == nullptr) throw std::invalid_argument("unexpected nullptr");
         const nsp::KernelChoice c = detail::seismic_autotune(
@@ -301,6 +311,7 @@ nsp_status_t nsp_index_autotune(nsp_index_t* index, int32_t n, const int32_t* in
         if (batch_docs != nullptr) *batch_docs = c.batch_docs;
         if (warps_per_block != nullptr) *warps_per_block = c.warps_per_block;
         if (kernel_ms != nullptr) *kernel_ms = c.kernel_ms;
+        if (ctas_per_query != nullptr) *ctas_per_query = c.split;
     });
 }
 

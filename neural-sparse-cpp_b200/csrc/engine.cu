@@ -522,14 +522,29 @@ struct SeismicPlan {
     int batch_docs;   // variants 2-5
     size_t smem_cta;  // variants 2-5
     int group_lanes;  // variants 2-5: lanes per scored doc
+    int cluster;      // variants 2-5: CTAs per query
+    int seg_cap;      // variants 2-5: block segments per batch
 };
+
+}  // namespace
+
+int auto_cluster(int n_queries) {
+    const int sms = device_sm_count();
+    int c = 1;
+    while (c < 8 && static_cast<long long>(std::max(n_queries, 1)) * (c * 2) <= sms) c *= 2;
+    return c;
+}
+
+namespace {
 
 // Variants 2-5 (one CTA per query). Warps per CTA: 8 when the batch has
 // queries enough to give every SM four CTAs; fewer queries get bigger CTAs
 // (16 or 32 warps, up to a whole SM per query), which shortens each query's
 // sequence of candidate batches -- the latency of small batches and of the
-// one-query-per-launch path. Candidate docs per batch: 64 per warp unless
-// asked otherwise; the batch shrinks if shared memory is short.
+// one-query-per-launch path -- and, below half a query per SM, a cluster of
+// 2-8 such CTAs per query (auto_cluster). Candidate docs per batch: 64 per
+// warp and CTA unless asked otherwise; the batch shrinks if shared memory is
+// short.
 SeismicPlan plan_seismic_cta(int kind, int dim, int qcap, int k, int n_queries,
                              const SeismicSearchArgs& args, bool single) {
     SeismicPlan p{};
@@ -543,19 +558,25 @@ SeismicPlan plan_seismic_cta(int kind, int dim, int qcap, int k, int n_queries,
         else if (per <= 2 * sms) warps = 16;
     }
     warps = std::min(std::max(warps, 1), 32);
-    int batch = args.batch_docs > 0 ? args.batch_docs : 64 * warps;
+    const int cl = args.cluster > 0 ? args.cluster : auto_cluster(single ? 1 : n_queries);
+    const int seg_cap = seismic_cta_seg_cap(cl);
+    int batch = args.batch_docs > 0 ? args.batch_docs : 64 * warps * cl;
     batch = std::min(std::max((batch + 31) & ~31, 32), 8192);
     const size_t limit = static_cast<size_t>(max_smem_optin());
-    while (batch > 32 && seismic_cta_smem(kind, dim, qcap, k, batch) > limit) batch >>= 1;
-    p.smem_cta = seismic_cta_smem(kind, dim, qcap, k, batch);
+    while (batch > 32 && seismic_cta_smem(kind, dim, qcap, k, batch, seg_cap) > limit) batch >>= 1;
+    p.smem_cta = seismic_cta_smem(kind, dim, qcap, k, batch, seg_cap);
     if (p.smem_cta > limit)
         throw std::invalid_argument("query too long or k too large for the device search kernel");
     p.batch_docs = batch;
     p.wpb = warps;
     p.group_lanes = 1 << std::min(std::max(args.variant - 2, 0), 3);  // 2..5 -> 1..8
+    p.cluster = cl;
+    p.seg_cap = seg_cap;
     int per_sm = seismic_cta_max_blocks_per_sm(kind, qcap, p.group_lanes, warps, p.smem_cta);
     if (per_sm < 1) per_sm = 1;
-    p.blocks = single ? 1 : std::max(1, std::min(n_queries, device_sm_count() * per_sm));
+    // whole clusters; a persistent grid of at most one resident wave
+    const int slots = std::max(1, device_sm_count() * per_sm / cl);
+    p.blocks = single ? cl : std::max(1, std::min(n_queries, slots)) * cl;
     return p;
 }
 
@@ -650,6 +671,8 @@ void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
         a.variant = args.variant;
         a.batch_docs = p.batch_docs;
         a.group_lanes = p.group_lanes;
+        a.cluster = p.cluster;
+        a.seg_cap = p.seg_cap;
         a.sel_q = args.d_sel_q;
         a.bscore = static_cast<float*>(ws.dev(
             Workspace::kBScore, static_cast<size_t>(p.blocks) * p.wpb * maxb * sizeof(float)));
@@ -681,7 +704,8 @@ void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
             for (int32_t q = 0; q < n; ++q) {
                 a.first_query = q;
                 a.q.n = q + 1;
-                cuda_check(launch_seismic_cta(kind, a, p.wpb, 1, s), "seismic search launch");
+                cuda_check(launch_seismic_cta(kind, a, p.wpb, p.blocks, s),
+                           "seismic search launch");
             }
             mark(e1);
             launches = n;

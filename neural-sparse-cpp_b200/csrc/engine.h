@@ -237,7 +237,14 @@ struct KernelChoice {
     int batch_docs = 0;
     int warps_per_block = 0;
     float kernel_ms = 0.0f;  // on the tuning sample
+    int split = 0;           // CTAs per query of one-query launches (0: the engine's rule)
 };
+
+// CTAs per query the engine gives a launch of `n_queries` queries: the most
+// of 1, 2, 4, 8 that still gives every query its own SMs (n * c <= SM count),
+// so a launch of few queries spreads each over a thread-block cluster; large
+// launches keep one CTA per query.
+int auto_cluster(int n_queries);
 
 struct SeismicSearchArgs {
     int k = 10;
@@ -253,6 +260,7 @@ struct SeismicSearchArgs {
                               // 2-5 one CTA per query with 1, 2, 4, 8 lanes per doc
     int stage_bytes = 0;      // staged: bytes per stage buffer (0 = default)
     int batch_docs = 0;       // variants 2-5: candidate docs per batch (0 = default)
+    int cluster = 0;          // variants 2-5: CTAs per query (0 = engine's choice, 1, 2, 4, 8)
     // variants 2-5: one device doc bitmap per query (a null entry admits every
     // doc), in device memory; replaces the launch-wide selector
     const uint64_t* const* d_sel_q = nullptr;

@@ -78,6 +78,7 @@ nsp::SeismicSearchArgs seismic_args(const SearchParameters* p, int k) {
         a.variant = p->engine.variant;
         a.stage_bytes = p->engine.stage_bytes;
         a.batch_docs = p->engine.batch_docs;
+        a.cluster = p->engine.ctas_per_query;
     }
     return a;
 }
@@ -357,6 +358,13 @@ const IDSelectorEnumerable* exact_match_selector(const IDSelector* sel, int k) {
 void apply_tuned(const SeismicState& st, nsp::SeismicSearchArgs& a, int64_t n_queries) {
     if (a.variant >= 0 || st.tuned.variant < 0) return;
     a.variant = st.tuned.variant;
+    if (a.cluster == 0 && st.tuned.split > 0) {
+        // the split measured fastest for a lone query, where the engine's
+        // rule would give a launch this small a cluster at all
+        const int rule = nsp::auto_cluster(
+            a.plain ? 1 : static_cast<int>(std::min<int64_t>(n_queries, 1 << 30)));
+        a.cluster = std::min(rule, st.tuned.split);
+    }
     if (a.plain || n_queries <= 2 * static_cast<int64_t>(nsp::device_sm_count())) return;
     if (a.batch_docs == 0) a.batch_docs = st.tuned.batch_docs;
     if (a.warps_per_block == 0) a.warps_per_block = st.tuned.warps_per_block;
@@ -703,6 +711,40 @@ nsp::KernelChoice seismic_autotune(Index* index, idx_t n, const idx_t* indptr,
                     best.kernel_ms = ms;
                 }
             }
+        }
+    }
+    // CTAs per query for one-query launches (the latency of a lone query):
+    // the fastest of 1, 2, 4, 8 over up to 16 of the sample's queries, each
+    // searched alone with the chosen lanes per doc
+    const int n1 = std::min<int>(n, 16);
+    float best_ms = 0.0f;
+    for (int split : {1, 2, 4, 8}) {
+        nsp::SeismicSearchArgs t = a;
+        t.variant = best.variant;
+        t.plain = true;
+        t.cluster = split;
+        float total = 0.0f;
+        for (int rep = 0; rep < 2; ++rep) {  // the first pass warms caches
+            total = 0.0f;
+            for (int i = 0; i < n1; ++i) {
+                nsp::QueryBatch one;
+                one.n = 1;
+                one.indptr = {0, q.ip[i + 1] - q.ip[i]};
+                one.idx.assign(q.ix + q.ip[i], q.ix + q.ip[i + 1]);
+                one.val.assign(q.vv + q.ip[i], q.vv + q.ip[i + 1]);
+                one.max_nnz = one.indptr[1];
+                one.ip = one.indptr.data();
+                one.ix = one.idx.data();
+                one.vv = one.val.data();
+                nsp::SearchStats s;
+                nsp::seismic_search(st->vectors.dev, st->lists_dev, one, t, nullptr, d.data(),
+                                    l.data(), &s);
+                total += s.kernel_ms;
+            }
+        }
+        if (best.split == 0 || total < best_ms) {
+            best.split = split;
+            best_ms = total;
         }
     }
     std::lock_guard<std::mutex> g(st->mu);

@@ -111,6 +111,11 @@ struct SeismicLaunch {
     int32_t order_stride;
     unsigned long long* sortkeys;
     int32_t sort_stride;
+    // Block segments a batch may hold, and CTAs per query: with cluster > 1
+    // each query runs on a thread-block cluster of that many CTAs, rank 0
+    // walking the query and every CTA scoring its batches.
+    int32_t seg_cap;
+    int32_t cluster;
 };
 
 struct ExactLaunch {
@@ -160,7 +165,9 @@ int seismic_max_blocks_per_sm(int val_kind, int variant, int warps_per_block, si
 int seismic_max_blocks_per_sm(int val_kind, int warps_per_block, size_t smem);  // variant 0
 
 // Variants 2-5: one CTA of `warps` warps per query (search_seismic_cta.cu).
-size_t seismic_cta_smem(int val_kind, int dim, int qcap, int k, int batch_docs);
+size_t seismic_cta_smem(int val_kind, int dim, int qcap, int k, int batch_docs, int seg_cap);
+// Block segments per batch the kernel is laid out for (more with a cluster).
+int seismic_cta_seg_cap(int cluster);
 int seismic_cta_max_blocks_per_sm(int val_kind, int qcap, int group_lanes, int warps,
                                   size_t smem);
 cudaError_t launch_seismic_cta(int val_kind, const SeismicLaunch& a, int warps, int blocks,

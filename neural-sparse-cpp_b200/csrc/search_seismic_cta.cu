@@ -40,6 +40,7 @@
 //      evicted or rejected scores <= the (monotone) heap minimum and is
 //      rejected again: the reference's visited set (seismic_index.cpp:104-
 //      107) without an O(n_docs) bitmap per query.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -53,11 +54,13 @@
 namespace nsp {
 namespace {
 
+namespace cg = cooperative_groups;
 using detail_search::heap_offer;
 using detail_search::kFull;
 using detail_search::ValT;
 
-constexpr int kSegCap = 128;  // block segments per batch
+constexpr int kSegCap = 128;    // block segments per batch, one CTA per query
+constexpr int kSegCapMax = 1024;  // the most any launch asks for (a cluster per query)
 
 // A run of consecutive docs of one block inside a batch.
 struct Seg {
@@ -81,13 +84,13 @@ struct Ctl {
 __host__ __device__ inline size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
 
 struct CtaLayout {
-    size_t tbl, qv, qterm, qraw, cuts, hs, hid, cdoc, coff, clen, csc, segs, total;
+    size_t tbl, qv, qterm, qraw, cuts, hs, hid, cdoc, coff, clen, csc, segs, cseg, total;
 };
 
 // Shared-memory layout of one CTA. The four candidate arrays are contiguous
 // (16 * batch bytes) and double as the sort-key buffer of the first list.
 __host__ __device__ inline CtaLayout cta_layout(int vsize, int tsize, int dim, int qcap, int k,
-                                                int batch) {
+                                                int batch, int seg_cap) {
     CtaLayout L;
     size_t o = a16(sizeof(Ctl));
     L.tbl = o;   o += a16(static_cast<size_t>(dim + 1) * tsize);
@@ -101,7 +104,8 @@ __host__ __device__ inline CtaLayout cta_layout(int vsize, int tsize, int dim, i
     L.coff = o;  o += static_cast<size_t>(batch) * 4;
     L.clen = o;  o += static_cast<size_t>(batch) * 4;
     L.csc = o;   o += static_cast<size_t>(batch) * 4;
-    L.segs = o;  o += static_cast<size_t>(kSegCap) * sizeof(Seg);
+    L.segs = o;  o += static_cast<size_t>(seg_cap) * sizeof(Seg);
+    L.cseg = o;  o += a16(static_cast<size_t>(batch) * 2);
     L.total = o;
     return L;
 }
@@ -346,6 +350,12 @@ __device__ void list_summaries(const SeismicLaunch& a, int t, int nb, const uint
                                const V* qraw, int qn, float* bscore, int lane,
                                unsigned long long& bytes) {
     constexpr int vsz = static_cast<int>(sizeof(V));
+    // uint8 codes: a block's score is a sum of at most qn products of two
+    // codes (<= 255 * 255 each), an integer below 2^24 -- exact in fp32 --
+    // while qn * 65025 < 2^24 (the reference sums these integer-valued floats
+    // in float as well, inverted_list_clusters.cpp:295-331)
+    const bool exact_any_order =
+        std::is_same<V, uint8_t>::value && static_cast<long long>(qn) * 65025ll < (1ll << 24);
     for (int b = lane; b < nb; b += 32) bscore[b] = 0.0f;
     __syncwarp();
     const uint2* meta = a.ix.lmeta + static_cast<size_t>(t) * a.ix.words;
@@ -378,12 +388,22 @@ __device__ void list_summaries(const SeismicLaunch& a, int t, int nb, const uint
             const float QV = __shfl_sync(kFull, qv, src);
             bytes += static_cast<unsigned long long>(R1 - R0) * (2 + vsz);
             const V* sv = static_cast<const V*>(a.ix.sval);
-            for (int64_t e = R0 + lane; e < R1; e += 32) {
-                const int blk = __ldg(a.ix.sblk + e);
-                const float p = __fmul_rn(QV, ValT<V>::f(__ldg(sv + e)));
-                bscore[blk] = __fadd_rn(bscore[blk], p);
+            if (exact_any_order) {
+                // integer products and sums below 2^24: every order of the
+                // float additions gives the same sum, so the updates need not
+                // wait for one another
+                for (int64_t e = R0 + lane; e < R1; e += 32) {
+                    const int blk = __ldg(a.ix.sblk + e);
+                    atomicAdd(bscore + blk, __fmul_rn(QV, ValT<V>::f(__ldg(sv + e))));
+                }
+            } else {
+                for (int64_t e = R0 + lane; e < R1; e += 32) {
+                    const int blk = __ldg(a.ix.sblk + e);
+                    const float p = __fmul_rn(QV, ValT<V>::f(__ldg(sv + e)));
+                    bscore[blk] = __fadd_rn(bscore[blk], p);
+                }
+                __syncwarp();
             }
-            __syncwarp();
         }
     }
 }
@@ -400,7 +420,7 @@ __device__ __forceinline__ unsigned long long order_key(float s, int b) {
 __device__ void sort_blocks(const float* bscore, int nb, unsigned long long* keys, int p2,
                             uint16_t* order, int tid, int nthreads) {
     for (int i = tid; i < p2; i += nthreads)
-        keys[i] = i < nb ? order_key(bscore[i], i) : ~0ull;
+        keys[i] = i < nb ? order_key(__ldcg(bscore + i), i) : ~0ull;
     __syncthreads();
     for (int k2 = 2; k2 <= p2; k2 <<= 1) {
         for (int j = k2 >> 1; j > 0; j >>= 1) {
@@ -439,7 +459,7 @@ struct Cursor {
 // receives the number of docs.
 __device__ int gather(const SeismicLaunch& a, Cursor& c, bool first, int64_t lb0, int nb,
                       const float* bscore, const uint16_t* order, int n, const float* hs,
-                      Seg* segs, int batch, int& total, int lane) {
+                      Seg* segs, int batch, int seg_cap, int& total, int lane) {
     int room = batch;
     int nseg = 0;
     total = 0;
@@ -465,14 +485,14 @@ __device__ int gather(const SeismicLaunch& a, Cursor& c, bool first, int64_t lb0
     }
     const bool full = n == a.k;
     const float hmin = full ? hs[a.k - 1] : 0.0f;
-    while (!c.split && !c.dead && room > 0 && nseg < kSegCap && c.o < nb) {
+    while (!c.split && !c.dead && room > 0 && nseg < seg_cap && c.o < nb) {
         const int p = c.o + lane;
         const bool in = p < nb;
         int blk = 0;
         float bs = 0.0f;
         if (in) {
             blk = first ? static_cast<int>(order[p]) : p;
-            bs = bscore[blk];
+            bs = __ldcg(bscore + blk);
         }
         const bool pass = in && !(full && __fmul_rn(bs, a.heap_factor) < hmin);
         const unsigned inm = __ballot_sync(kFull, in);
@@ -502,7 +522,7 @@ __device__ int gather(const SeismicLaunch& a, Cursor& c, bool first, int64_t lb0
         const int excl = incl - sz;
         const unsigned cm = __ballot_sync(kFull, cand);
         const int r = __popc(cm & ((1u << lane) - 1u));
-        const bool take = cand && excl < room && nseg + r < kSegCap;
+        const bool take = cand && excl < room && nseg + r < seg_cap;
         const unsigned tm = __ballot_sync(kFull, take);
         if (take) {
             Seg g;
@@ -550,7 +570,17 @@ __device__ int gather(const SeismicLaunch& a, Cursor& c, bool first, int64_t lb0
     return nseg;
 }
 
-template <typename V, typename TE, int kG>
+// A cluster's CTAs meet here (barrier.cluster arrive + wait: release and
+// acquire of shared memory across the cluster).
+__device__ __forceinline__ void cluster_sync() { cg::this_cluster().sync(); }
+
+// The leader writes a control word into every other CTA of its cluster.
+__device__ __forceinline__ void push_to_cluster(int32_t* field, int32_t v) {
+    cg::cluster_group cl = cg::this_cluster();
+    for (unsigned r = 1; r < cl.num_blocks(); ++r) *cl.map_shared_rank(field, r) = v;
+}
+
+template <typename V, typename TE, int kG, bool kCl>
 __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr bool kRank = std::is_same<V, float>::value;
@@ -561,7 +591,8 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
     const int nwarps = blockDim.x >> 5;
     const int dim = a.fwd.dim;
     const int batch = a.batch_docs;
-    const CtaLayout L = cta_layout(vsz, static_cast<int>(sizeof(TE)), dim, a.qcap, a.k, batch);
+    const CtaLayout L =
+        cta_layout(vsz, static_cast<int>(sizeof(TE)), dim, a.qcap, a.k, batch, a.seg_cap);
     Ctl* ctl = reinterpret_cast<Ctl*>(smem);
     TE* tbl = reinterpret_cast<TE*>(smem + L.tbl);
     float* qv = reinterpret_cast<float*>(smem + L.qv);
@@ -575,6 +606,7 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
     uint32_t* clen = reinterpret_cast<uint32_t*>(smem + L.clen);
     float* csc = reinterpret_cast<float*>(smem + L.csc);
     Seg* segs = reinterpret_cast<Seg*>(smem + L.segs);
+    uint16_t* cseg = reinterpret_cast<uint16_t*>(smem + L.cseg);  // each candidate's segment
 
     const int maxb = a.ix.max_blocks;
     float* bscore_cta = a.bscore + static_cast<size_t>(blockIdx.x) * nwarps * maxb;
@@ -586,6 +618,77 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
     for (int i = tid; i <= dim; i += blockDim.x) tbl[i] = 0;
     if (tid == 0) qv[0] = 0.0f;
 
+    // With a cluster per query, the scoring phase of every CTA claims the
+    // leader's (rank 0) candidates and writes the scores back there; the
+    // pointers below are the leader's arrays as the cluster addresses them.
+    Ctl* sctl = ctl;
+    const uint32_t* scoff = coff;
+    const uint32_t* sclen = clen;
+    float* scsc = csc;
+    unsigned cid = blockIdx.x, ncl = gridDim.x;  // this CTA's query slot, and the slots
+    if constexpr (kCl) {
+        cg::cluster_group cl = cg::this_cluster();
+        sctl = cl.map_shared_rank(ctl, 0);
+        scoff = cl.map_shared_rank(coff, 0);
+        sclen = cl.map_shared_rank(clen, 0);
+        scsc = cl.map_shared_rank(csc, 0);
+        asm("mov.u32 %0, %%clusterid.x;" : "=r"(cid));
+        asm("mov.u32 %0, %%nclusterid.x;" : "=r"(ncl));
+        // every CTA of the cluster runs before any touches another's memory
+        __syncthreads();
+        cluster_sync();
+        if (cl.block_rank() != 0) {
+            // A scoring CTA: per query, the leader publishes the query index
+            // (q >= n: none left), then each batch's candidate count (-1:
+            // the query is done); barriers pair one to one with the leader's.
+            for (;;) {
+                __syncthreads();
+                cluster_sync();
+                const int q = ctl->q;
+                if (q >= a.q.n) break;
+                const int32_t qs = a.q.indptr[q];
+                int qn = a.q.indptr[q + 1] - qs;
+                if (qn > a.qcap || qn < 0) qn = 0;  // the leader reports it
+                bool bad = false;
+                for (int i = tid; i < qn; i += blockDim.x) {
+                    const uint32_t t = a.q.idx[qs + i];
+                    const V v = static_cast<const V*>(a.q.val)[qs + i];
+                    qterm[i] = static_cast<uint16_t>(t);
+                    if (t < static_cast<uint32_t>(dim)) {
+                        if constexpr (kRank) {
+                            tbl[t] = static_cast<TE>(i + 1);
+                        } else {
+                            tbl[t] = static_cast<TE>(v);
+                        }
+                    }
+                    if constexpr (kRank) {
+                        qv[i + 1] = ValT<V>::f(v);
+                        bad |= !isfinite(ValT<V>::f(v));
+                    }
+                }
+                const bool nonfinite = __syncthreads_or(bad) != 0;
+                for (;;) {
+                    cluster_sync();
+                    const int total = ctl->total;
+                    if (total < 0) break;
+                    if (kRank && nonfinite)
+                        score_batch<V, TE, true, kG>(a.fwd, sctl, tbl, qv, scoff, sclen, scsc,
+                                                     total, lane);
+                    else
+                        score_batch<V, TE, false, kG>(a.fwd, sctl, tbl, qv, scoff, sclen, scsc,
+                                                      total, lane);
+                    cluster_sync();
+                }
+                __syncthreads();
+                for (int i = tid; i < qn; i += blockDim.x) {
+                    const uint32_t t = qterm[i];
+                    if (t < static_cast<uint32_t>(dim)) tbl[t] = 0;
+                }
+            }
+            return;
+        }
+    }
+
     int iter = 0;
     for (;;) {
         if (tid == 0) {
@@ -593,11 +696,13 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
             if (a.work_counter != nullptr)
                 q = atomicAdd(a.work_counter, 1);
             else
-                q = a.first_query + blockIdx.x + iter * gridDim.x;
+                q = a.first_query + static_cast<int>(cid) + iter * static_cast<int>(ncl);
             ctl->q = q;
+            if constexpr (kCl) push_to_cluster(&ctl->q, q);
         }
         ++iter;
         __syncthreads();
+        if constexpr (kCl) cluster_sync();
         const int q = ctl->q;
         if (q >= a.q.n) break;
 
@@ -701,7 +806,7 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                     if (warp == 0) {
                         int total = 0;
                         const int nseg = gather(a, cur, first, lb0, nb, bscore, order, n, hs,
-                                                segs, batch, total, lane);
+                                                segs, batch, a.seg_cap, total, lane);
                         if (lane == 0) {
                             ctl->nseg = nseg;
                             ctl->total = total;
@@ -736,35 +841,40 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                             cdoc[i] = member ? d : -1;
                             coff[i] = ri.x;
                             clen[i] = ri.y;
+                            cseg[i] = static_cast<uint16_t>(lo);
                         }
                         __syncthreads();
-                        // 6. scores
-                        if constexpr (kRank) {
-                            if (nonfinite)
-                                score_batch<V, TE, true, kG>(a.fwd, ctl, tbl, qv, coff, clen, csc,
-                                                             total, lane);
-                            else
-                                score_batch<V, TE, false, kG>(a.fwd, ctl, tbl, qv, coff, clen,
-                                                              csc, total, lane);
-                        } else {
-                            score_batch<V, TE, false, kG>(a.fwd, ctl, tbl, qv, coff, clen, csc,
-                                                          total, lane);
+                        // 6. scores (with the cluster's other CTAs)
+                        if constexpr (kCl) {
+                            if (tid == 0) push_to_cluster(&ctl->total, total);
+                            cluster_sync();
                         }
+                        if (kRank && nonfinite)
+                            score_batch<V, TE, true, kG>(a.fwd, sctl, tbl, qv, scoff, sclen, scsc,
+                                                         total, lane);
+                        else
+                            score_batch<V, TE, false, kG>(a.fwd, sctl, tbl, qv, scoff, sclen,
+                                                          scsc, total, lane);
+                        if constexpr (kCl) cluster_sync();
                         __syncthreads();
                     }
                     // 7. second pruning test and heap offers, in block order
                     if (warp == 0) {
-                        for (int s = 0; s < nseg; ++s) {
+                        // One segment exactly as the reference walks it: the
+                        // block's test against the heap as it stands, then
+                        // its docs offered in order. True when the first
+                        // list's walk ends here.
+                        auto walk_segment = [&](int s) -> bool {
                             const Seg g = segs[s];
                             if (g.head) {
                                 if (n == a.k && __fmul_rn(g.bs, a.heap_factor) < hs[a.k - 1]) {
                                     if (first) {
                                         cur.dead = true;
                                         cur.split = false;
-                                        break;
+                                        return true;
                                     }
                                     if (s == nseg - 1) cur.split = false;
-                                    continue;
+                                    return false;
                                 }
                                 ++blocks_visited;
                                 bytes += 16;
@@ -793,6 +903,75 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                                     heap_offer(S, D, hs, hid, n, a.k, lane);
                                 }
                             }
+                            return false;
+                        };
+                        // Windows of whole segments with at most 32 docs in
+                        // all, one doc per lane. While the heap is full and no
+                        // doc of a window beats its minimum, walking the
+                        // window changes nothing in the heap, so every block
+                        // test in it sees the same minimum: one pass settles
+                        // the window. Otherwise (or for a larger segment) the
+                        // window is walked segment by segment.
+                        int s = 0;
+                        while (s < nseg) {
+                            const int base = segs[s].cand0;
+                            const int sl = s + lane;
+                            const bool valid = sl < nseg;
+                            int end = INT_MAX, head = 0, cnt = 0;
+                            float bs = 0.0f;
+                            if (valid) {
+                                const Seg g = segs[sl];
+                                end = g.cand0 + g.cnt - base;
+                                head = g.head;
+                                cnt = g.cnt;
+                                bs = g.bs;
+                            }
+                            // segment ends grow with the index: a prefix fits
+                            const int w = __popc(__ballot_sync(kFull, valid && end <= 32));
+                            bool stop = false;
+                            if (w == 0 || n < a.k) {
+                                const int e = w == 0 ? s + 1 : s + w;
+                                for (int t = s; t < e && !stop; ++t) stop = walk_segment(t);
+                                if (stop) break;
+                                s = e;
+                                continue;
+                            }
+                            const float hmin = hs[a.k - 1];
+                            const bool fail =
+                                lane < w && head && __fmul_rn(bs, a.heap_factor) < hmin;
+                            const unsigned failm = __ballot_sync(kFull, fail);
+                            // the first list ends at its first failing block
+                            const int wl = (first && failm) ? __ffs(failm) - 1 : w;
+                            const int ndocs = wl > 0 ? __shfl_sync(kFull, end, wl - 1) : 0;
+                            bool mem = false;
+                            float sc = 0.0f;
+                            if (lane < ndocs) {
+                                const int rs = static_cast<int>(cseg[base + lane]) - s;
+                                mem = !((failm >> rs) & 1u) && cdoc[base + lane] >= 0;
+                                sc = csc[base + lane];
+                            }
+                            if (__any_sync(kFull, mem && sc > hmin)) {
+                                for (int t = s; t < s + w && !stop; ++t) stop = walk_segment(t);
+                                if (stop) break;
+                                s += w;
+                                continue;
+                            }
+                            const bool took = lane < wl && !fail;
+                            const unsigned heads = __ballot_sync(kFull, took && head);
+                            blocks_visited += __popc(heads);
+                            bytes += 16ull * __popc(heads) +
+                                     4ull * __reduce_add_sync(kFull, took ? cnt : 0);
+                            if (mem)
+                                lane_bytes += 8ull + static_cast<unsigned long long>(
+                                                         clen[base + lane]) * (2 + vsz);
+                            docs_scored += __popc(__ballot_sync(kFull, mem));
+                            if (wl < w) {
+                                cur.dead = true;
+                                cur.split = false;
+                                break;
+                            }
+                            if (s + w == nseg && ((failm >> (w - 1)) & 1u)) cur.split = false;
+                            s += w;
                         }
                     }
                 }
@@ -800,6 +979,11 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
             first = false;  // seismic_index.cpp:261
         }
 
+        if constexpr (kCl) {  // the query is done: the scoring CTAs move on
+            __syncthreads();
+            if (tid == 0) push_to_cluster(&ctl->total, -1);
+            cluster_sync();
+        }
         // results, padded with (-1.0, -1); SQ scores decoded
         // (seismic_scalar_quantized_index.cpp:345-355)
         if (warp == 0) {
@@ -838,18 +1022,18 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
 }
 
 template <typename V, typename TE>
-size_t smem_typed(int dim, int qcap, int k, int batch) {
+size_t smem_typed(int dim, int qcap, int k, int batch, int seg_cap) {
     return cta_layout(static_cast<int>(sizeof(V)), static_cast<int>(sizeof(TE)), dim, qcap, k,
-                      batch)
+                      batch, seg_cap)
         .total;
 }
 
 template <typename V, typename TE, int kG>
 int max_blocks_cta_g(int threads, size_t smem) {
-    if (allow_opt_in_smem(seismic_cta_kernel<V, TE, kG>) != cudaSuccess)
+    if (allow_opt_in_smem(seismic_cta_kernel<V, TE, kG, false>) != cudaSuccess)
         return 0;
     int blocks = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, seismic_cta_kernel<V, TE, kG>,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, seismic_cta_kernel<V, TE, kG, false>,
                                                       threads, smem) != cudaSuccess)
         return 0;
     return blocks;
@@ -866,15 +1050,34 @@ int max_blocks_cta_typed(int group, int threads, size_t smem) {
 template <typename V, typename TE, int kG>
 cudaError_t launch_cta_g(const SeismicLaunch& a, int warps, int blocks, size_t smem,
                          cudaStream_t s) {
-    cudaError_t e = allow_opt_in_smem(seismic_cta_kernel<V, TE, kG>);
+    if (a.cluster > 1) {
+        // one cluster of a.cluster CTAs per query; the grid is whole clusters
+        auto* f = seismic_cta_kernel<V, TE, kG, true>;
+        cudaError_t e = allow_opt_in_smem(f);
+        if (e != cudaSuccess) return e;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(static_cast<unsigned>(blocks));
+        cfg.blockDim = dim3(static_cast<unsigned>(warps * 32));
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = static_cast<unsigned>(a.cluster);
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, f, a);
+    }
+    cudaError_t e = allow_opt_in_smem(seismic_cta_kernel<V, TE, kG, false>);
     if (e != cudaSuccess) return e;
-    seismic_cta_kernel<V, TE, kG><<<blocks, warps * 32, smem, s>>>(a);
+    seismic_cta_kernel<V, TE, kG, false><<<blocks, warps * 32, smem, s>>>(a);
     return cudaGetLastError();
 }
 
 template <typename V, typename TE>
 cudaError_t launch_cta_typed(const SeismicLaunch& a, int warps, int blocks, cudaStream_t s) {
-    const size_t smem = smem_typed<V, TE>(a.fwd.dim, a.qcap, a.k, a.batch_docs);
+    const size_t smem = smem_typed<V, TE>(a.fwd.dim, a.qcap, a.k, a.batch_docs, a.seg_cap);
     if (a.group_lanes == 8) return launch_cta_g<V, TE, 8>(a, warps, blocks, smem, s);
     if (a.group_lanes == 4) return launch_cta_g<V, TE, 4>(a, warps, blocks, smem, s);
     if (a.group_lanes == 2) return launch_cta_g<V, TE, 2>(a, warps, blocks, smem, s);
@@ -889,13 +1092,16 @@ static bool wide_table(int val_kind, int qcap) {
     return val_kind == kU16 || (val_kind == kF32 && qcap > 255);
 }
 
-size_t seismic_cta_smem(int val_kind, int dim, int qcap, int k, int batch) {
+size_t seismic_cta_smem(int val_kind, int dim, int qcap, int k, int batch, int seg_cap) {
     if (val_kind == kF32)
-        return wide_table(val_kind, qcap) ? smem_typed<float, uint16_t>(dim, qcap, k, batch)
-                                          : smem_typed<float, uint8_t>(dim, qcap, k, batch);
-    if (val_kind == kU8) return smem_typed<uint8_t, uint8_t>(dim, qcap, k, batch);
-    return smem_typed<uint16_t, uint16_t>(dim, qcap, k, batch);
+        return wide_table(val_kind, qcap)
+                   ? smem_typed<float, uint16_t>(dim, qcap, k, batch, seg_cap)
+                   : smem_typed<float, uint8_t>(dim, qcap, k, batch, seg_cap);
+    if (val_kind == kU8) return smem_typed<uint8_t, uint8_t>(dim, qcap, k, batch, seg_cap);
+    return smem_typed<uint16_t, uint16_t>(dim, qcap, k, batch, seg_cap);
 }
+
+int seismic_cta_seg_cap(int cluster) { return cluster > 1 ? kSegCapMax : kSegCap; }
 
 int seismic_cta_max_blocks_per_sm(int val_kind, int qcap, int group, int warps, size_t smem) {
     const int th = warps * 32;

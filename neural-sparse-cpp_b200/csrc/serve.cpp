@@ -244,6 +244,7 @@ void Server::worker() {
         std::vector<std::shared_ptr<ServerRequest>> batch;
         std::vector<const uint64_t*> sel;
         int64_t est = 0;
+        int64_t others = 0;  // queries other workers have on the GPU
         {
             std::unique_lock<std::mutex> lk(mu_);
             cv_work_.wait(lk, [&] {
@@ -270,6 +271,8 @@ void Server::worker() {
             }
             n_pending_ -= static_cast<int64_t>(batch.size());
             in_use_ += est;
+            others = in_flight_queries_;
+            in_flight_queries_ += static_cast<int64_t>(batch.size());
             sel.assign(batch.size(), nullptr);
             for (size_t i = 0; i < batch.size(); ++i)
                 if (batch[i]->filter >= 0)
@@ -300,6 +303,12 @@ void Server::worker() {
             SeismicSearchParameters params(batch[0]->cut, batch[0]->hf);
             nsp::SeismicSearchArgs a;
             resolve_seismic(index_, &params, k, a);
+            // CTAs per query by the queries on the GPU at once, this batch's
+            // and the other workers': a cluster per query only while the SMs
+            // would otherwise idle (capped by the autotuner's split)
+            a.cluster = std::min(
+                nsp::auto_cluster(static_cast<int>(std::min<int64_t>(others + n, 1 << 30))),
+                st_->tuned.split > 0 ? st_->tuned.split : 8);
             apply_tuned(*st_, a, static_cast<int64_t>(batch.size()));
             if (a.variant >= 0 && a.variant < 2) a.variant = -1;  // needs one CTA per query
             const bool any =
@@ -336,6 +345,7 @@ void Server::worker() {
                 r.done = true;
             }
             in_use_ -= est;
+            in_flight_queries_ -= n;
         }
         cv_done_.notify_all();
         cv_work_.notify_all();

@@ -109,6 +109,7 @@ private:
     std::unordered_map<int64_t, std::shared_ptr<ServerRequest>> live_;
     int64_t next_ticket_ = 0;
     int64_t in_use_ = 0;
+    int64_t in_flight_queries_ = 0;  // queries of the launches running now
     bool stop_ = false;
     ServerStats stats_;
     std::vector<std::thread> workers_;

@@ -71,11 +71,13 @@ _sig("nsp_seismic_sq_search_params_new", ctypes.c_float, ctypes.c_float, ctypes.
 _sig("nsp_search_params_set_id_selector", _P, _P)
 _sig("nsp_search_params_set_engine", _P, ctypes.c_int, ctypes.c_int)
 _sig("nsp_search_params_set_kernel", _P, ctypes.c_int, ctypes.c_int)
+_sig("nsp_search_params_set_split", _P, ctypes.c_int)
 _sig("nsp_search_params_free", _P)
 _sig("nsp_index_search_device", _P, _I32, _P, _P, _P, _I32, ctypes.c_int, _P, _P, _P, _P)
 _sig("nsp_device_info", ctypes.POINTER(_I32), ctypes.c_char_p, ctypes.c_size_t)
 _sig("nsp_index_autotune", _P, _I32, _P, _P, _P, ctypes.c_int, _P, ctypes.POINTER(ctypes.c_int),
-     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float))
+     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float),
+     ctypes.POINTER(ctypes.c_int))
 
 
 class _Stats(ctypes.Structure):
@@ -196,6 +198,11 @@ class SearchParameters:
         default). Results do not depend on either."""
         _check(_L.nsp_search_params_set_kernel(self._h, int(variant), int(tuning)))
 
+    def set_split(self, ctas_per_query=0):
+        """Extension: CTAs per query of SEISMIC variants 2-5 (0 auto, 1, or a
+        cluster of 2, 4 or 8 CTAs scoring each query together)."""
+        _check(_L.nsp_search_params_set_split(self._h, int(ctas_per_query)))
+
     def __del__(self):
         h, self._h = getattr(self, "_h", None), None
         if h:
@@ -284,14 +291,14 @@ class Index:
         indptr = np.ascontiguousarray(indptr, dtype=np.int32)
         indices = np.ascontiguousarray(indices, dtype=np.uint16)
         values = np.ascontiguousarray(values, dtype=np.float32)
-        v, b, w = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        v, b, w, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         ms = ctypes.c_float()
         _check(_L.nsp_index_autotune(self._h, int(n), _ptr(indptr), _ptr(indices), _ptr(values),
                                      int(k), None if params is None else params._h,
                                      ctypes.byref(v), ctypes.byref(b), ctypes.byref(w),
-                                     ctypes.byref(ms)))
+                                     ctypes.byref(ms), ctypes.byref(c)))
         return {"variant": v.value, "batch_docs": b.value, "warps_per_block": w.value,
-                "kernel_ms": ms.value}
+                "kernel_ms": ms.value, "ctas_per_query": c.value}
 
     def num_vectors(self):
         out = ctypes.c_int64()

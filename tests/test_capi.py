@@ -161,6 +161,11 @@ def test_kernel_and_engine_knobs_are_validated():
     p.set_engine(False, 32)
     with pytest.raises(ValueError):
         p.set_engine(False, 33)
+    for split in (0, 1, 2, 4, 8):
+        p.set_split(split)
+    for split in (-1, 3, 16):
+        with pytest.raises(ValueError):
+            p.set_split(split)
 
 
 def test_autotune_and_server_need_a_seismic_index():

@@ -256,9 +256,16 @@ def test_autotune_picks_a_shape_and_keeps_results(seismic_file):
     c = idx.autotune(qs.n, qs.indptr, qs.indices, qs.values, K, p)
     assert 2 <= c["variant"] <= 5 and c["batch_docs"] in (256, 512, 1024)
     assert c["warps_per_block"] in (4, 8) and c["kernel_ms"] > 0
+    assert c["ctas_per_query"] in (1, 2, 4, 8)
     D1, L1 = search(idx, qs, params=p)
     np.testing.assert_array_equal(L1, L0)
     np.testing.assert_array_equal(D1, D0)
+    # one-query launches take the tuned split
+    p1 = nsparse.SeismicSearchParameters(CUT, HF)
+    p1.set_engine(plain=True)
+    D2, L2 = search(idx, qs.rows(0, 8), params=p1)
+    np.testing.assert_array_equal(L2, L0[:8])
+    np.testing.assert_array_equal(D2, D0[:8])
 
 
 def test_seismic_filter_and_exact_path_match_golden(seismic_file):
