@@ -558,13 +558,21 @@ SeismicPlan plan_seismic_cta(int kind, int dim, int qcap, int k, int n_queries,
         else if (per <= 2 * sms) warps = 16;
     }
     warps = std::min(std::max(warps, 1), 32);
-    const int cl = args.cluster > 0 ? args.cluster : auto_cluster(single ? 1 : n_queries);
-    const int seg_cap = seismic_cta_seg_cap(cl);
-    int batch = args.batch_docs > 0 ? args.batch_docs : 64 * warps * cl;
-    batch = std::min(std::max((batch + 31) & ~31, 32), 8192);
     const size_t limit = static_cast<size_t>(max_smem_optin());
-    while (batch > 32 && seismic_cta_smem(kind, dim, qcap, k, batch, seg_cap) > limit) batch >>= 1;
-    p.smem_cta = seismic_cta_smem(kind, dim, qcap, k, batch, seg_cap);
+    int cl = args.cluster > 0 ? args.cluster : auto_cluster(single ? 1 : n_queries);
+    int seg_cap = 0, batch = 0;
+    for (;;) {
+        seg_cap = seismic_cta_seg_cap(cl);
+        batch = args.batch_docs > 0 ? args.batch_docs : 64 * warps * cl;
+        batch = std::min(std::max((batch + 31) & ~31, 32), 8192);
+        while (batch > 32 && seismic_cta_smem(kind, dim, qcap, k, batch, seg_cap) > limit)
+            batch >>= 1;
+        p.smem_cta = seismic_cta_smem(kind, dim, qcap, k, batch, seg_cap);
+        // a cluster's larger segment table must not cost the engine's own
+        // choice a query it could run on one CTA
+        if (p.smem_cta <= limit || args.cluster > 0 || cl == 1) break;
+        cl = 1;
+    }
     if (p.smem_cta > limit)
         throw std::invalid_argument("query too long or k too large for the device search kernel");
     p.batch_docs = batch;
