@@ -1067,7 +1067,19 @@ cudaError_t launch_cta_g(const SeismicLaunch& a, int warps, int blocks, size_t s
         at[0].val.clusterDim.z = 1;
         cfg.attrs = at;
         cfg.numAttrs = 1;
-        return cudaLaunchKernelEx(&cfg, f, a);
+        int fits = 0;
+        if (cudaOccupancyMaxActiveClusters(&fits, f, &cfg) == cudaSuccess && fits > 0)
+            return cudaLaunchKernelEx(&cfg, f, a);
+        // A device that cannot place such a cluster runs the query on one CTA
+        // (same results): the same grid walks the same queries, the extra
+        // CTAs of a one-query launch find none left.
+        (void)cudaGetLastError();
+        SeismicLaunch one = a;
+        one.cluster = 1;
+        e = allow_opt_in_smem(seismic_cta_kernel<V, TE, kG, false>);
+        if (e != cudaSuccess) return e;
+        seismic_cta_kernel<V, TE, kG, false><<<blocks, warps * 32, smem, s>>>(one);
+        return cudaGetLastError();
     }
     cudaError_t e = allow_opt_in_smem(seismic_cta_kernel<V, TE, kG, false>);
     if (e != cudaSuccess) return e;
