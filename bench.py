@@ -166,10 +166,30 @@ def cpu_baseline(docs, qs, index_file, sample):
     t = time.perf_counter()
     r.search(q, K, param_kind=2, cut=CUT, heap_factor=HF)
     dt = time.perf_counter() - t
+    lat = ref_per_query_latency(L, r, q, min(200, sample), cores)
     r.close()
     return {"value": sample / dt, "unit": "queries/s", "cores": cores, "kind": "reference",
             "sample": f"{sample} of the {N_QUERIES} queries, one batched search() call, "
-                      f"reference {variant} build, OMP threads={cores}"}
+                      f"reference {variant} build, OMP threads={cores}",
+            "per_query_1_thread": lat}
+
+
+def ref_per_query_latency(L, r, q, n, cores):
+    """The reference's per-query latency as its residency benchmark takes it
+    (benchmarks/sq_residency_bench.cpp:249-269): one thread, one search() call
+    per query, wall time of each call; p50/p99 over the first n queries."""
+    L.ref_set_threads(1)
+    try:
+        ms = []
+        for i in range(n):
+            one = q.rows(i, i + 1)
+            t = time.perf_counter()
+            r.search(one, K, param_kind=2, cut=CUT, heap_factor=HF)
+            ms.append(1000.0 * (time.perf_counter() - t))
+    finally:
+        L.ref_set_threads(cores)
+    return {"queries": n, "p50_ms": float(np.percentile(ms, 50)),
+            "p99_ms": float(np.percentile(ms, 99)), "threads": 1}
 
 
 def ref_variant():
@@ -209,6 +229,7 @@ def run_reference(args):
         r.search(q, K, param_kind=2, cut=CUT, heap_factor=HF)
         times.append(time.perf_counter() - t)
     value = sample * len(times) / sum(times)
+    lat = ref_per_query_latency(O.ref_lib(variant), r, q, 200, cores)
     out = {"metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": 0, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": 1000 * sum(times) / len(times),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -216,7 +237,8 @@ def run_reference(args):
            "build_s": build_s,
            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cores, "kind": "reference",
                             "sample": f"{sample} queries per step, one batched search() call, "
-                                      f"reference {variant} build"},
+                                      f"reference {variant} build",
+                            "per_query_1_thread": lat},
            "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
@@ -619,15 +641,25 @@ def run_engine_brutal(args):
     idx.add(docs.n, docs.indptr, docs.indices, docs.values)
     for _ in range(max(args.warmup, 3)):
         idx.search(qs.n, qs.indptr, qs.indices, qs.values, K)
-    times, kms = [], []
+    # the postings (8 B per nonzero) fit in L2 at 100k docs: flush it before
+    # every timed step
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    times, kms, nbytes, launches = [], [], [], 0
     for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
         t = time.perf_counter()
         D, L = idx.search(qs.n, qs.indptr, qs.indices, qs.values, K)
         times.append(time.perf_counter() - t)
-        kms.append(nsparse.last_search_stats().kernel_ms)
+        st = nsparse.last_search_stats()
+        kms.append(st.kernel_ms)
+        nbytes.append(st.bytes)
+        launches += st.launches
     value = qs.n * len(times) / sum(times)
     kernel_ms = statistics.median(kms)
     bytes_ = 4 * (docs.n + 1) + 6 * docs.nnz  # forward index read once per launch
+    algo = statistics.median(nbytes)  # postings of the queries' terms, counted by the kernel
+    peak, peak_src = measured_peaks()
     cpu = None
     variant = ref_variant()
     if variant is not None and not args.no_cpu:
@@ -649,10 +681,16 @@ def run_engine_brutal(args):
         "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
         "ms_per_step": 1000 * sum(times) / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"brutal_fp32_{docs.n}_docs_{qs.n}_queries", "k": K},
+        "config": {"workload": f"brutal_fp32_{docs.n}_docs_{qs.n}_queries", "k": K,
+                   "l2": "flushed between steps", "kernel": "term at a time (exact_taat_kernel)"},
         "kernel_ms_per_launch": kernel_ms,
         "kernel_queries_per_s": qs.n / (kernel_ms / 1000.0),
         "forward_index_gbs": bytes_ / (kernel_ms / 1000.0) / 1e9,
+        "roofline": {"bound": "hbm", "achieved": algo / (kernel_ms / 1000.0) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": algo / (kernel_ms / 1000.0) / 1e9 / peak,
+                     "peak_source": peak_src, "traffic": None,
+                     "algorithmic_bytes_per_launch": algo},
+        "gpu_launches": launches,
         "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step":
                 4 * (qs.n + 1) + 6 * qs.nnz, "d2h_bytes_per_step": qs.n * K * 8},
         "cpu_baseline": cpu}))

@@ -859,8 +859,8 @@ void seismic_search_device(const ForwardDevice& fwd, const SeismicDevice& ix, in
                 stats);
 }
 
-void exact_search(const ForwardDevice& fwd, const QueryBatch& q, int k, int mode,
-                  const std::vector<uint64_t>* sel_bits, float* out_d, int32_t* out_l,
+void exact_search(const ForwardDevice& fwd, const PostingsDevice* post, const QueryBatch& q, int k,
+                  int mode, const std::vector<uint64_t>* sel_bits, float* out_d, int32_t* out_l,
                   SearchStats* stats) {
     Workspace& ws = Workspace::get();
     cudaStream_t s = ws.stream();
@@ -882,10 +882,12 @@ void exact_search(const ForwardDevice& fwd, const QueryBatch& q, int k, int mode
     a.qcap = std::max(q.max_nnz, 1);
     a.out_d = dd;
     a.out_l = dl;
+    const bool taat = post != nullptr && post->usable() &&
+                      post->generation() == fwd.generation() && k <= kTaatMaxK;
     const int words = (fwd.view().dim + 31) / 32;
     const size_t limit = static_cast<size_t>(max_smem_optin());
     const bool values_global = exact_smem(words, a.qcap) > limit;
-    if (exact_smem(words, 0) > limit)
+    if (!taat && exact_smem(words, 0) > limit)
         throw std::invalid_argument("vocabulary too large for the exact search kernel");
     const int groups = (q.n + 31) / 32;
     const int sms = device_sm_count();
@@ -894,17 +896,25 @@ void exact_search(const ForwardDevice& fwd, const QueryBatch& q, int k, int mode
     tiles = std::min(tiles, std::max(1, nd / 64));
     a.docs_per_tile = (nd + tiles - 1) / tiles;
     tiles = (nd + a.docs_per_tile - 1) / a.docs_per_tile;
-    const size_t lanes = static_cast<size_t>(groups) * tiles * 8 * 32;
-    a.heap_d = static_cast<float*>(ws.dev(Workspace::kHeapD, lanes * k * sizeof(float)));
-    a.heap_l = static_cast<int32_t*>(ws.dev(Workspace::kHeapL, lanes * k * sizeof(int32_t)));
-    const size_t cands = static_cast<size_t>(groups) * 32 * tiles * k;
-    a.cand_d = static_cast<float*>(ws.dev(Workspace::kCandD, cands * sizeof(float)));
-    a.cand_l = static_cast<int32_t*>(ws.dev(Workspace::kCandL, cands * sizeof(int32_t)));
-    a.qval_global = values_global
-                        ? static_cast<float*>(ws.dev(Workspace::kQValG,
-                                                     static_cast<size_t>(groups) * tiles * 32 *
-                                                         a.qcap * sizeof(float)))
-                        : nullptr;
+    if (taat) {
+        // term at a time: candidates per (query, doc chunk), no per-lane lists
+        a.post = post->view();
+        const size_t cands = static_cast<size_t>(q.n) * a.post.n_chunks * k;
+        a.cand_d = static_cast<float*>(ws.dev(Workspace::kCandD, cands * sizeof(float)));
+        a.cand_l = static_cast<int32_t*>(ws.dev(Workspace::kCandL, cands * sizeof(int32_t)));
+    } else {
+        const size_t lanes = static_cast<size_t>(groups) * tiles * 8 * 32;
+        a.heap_d = static_cast<float*>(ws.dev(Workspace::kHeapD, lanes * k * sizeof(float)));
+        a.heap_l = static_cast<int32_t*>(ws.dev(Workspace::kHeapL, lanes * k * sizeof(int32_t)));
+        const size_t cands = static_cast<size_t>(groups) * 32 * tiles * k;
+        a.cand_d = static_cast<float*>(ws.dev(Workspace::kCandD, cands * sizeof(float)));
+        a.cand_l = static_cast<int32_t*>(ws.dev(Workspace::kCandL, cands * sizeof(int32_t)));
+        a.qval_global = values_global
+                            ? static_cast<float*>(ws.dev(Workspace::kQValG,
+                                                         static_cast<size_t>(groups) * tiles * 32 *
+                                                             a.qcap * sizeof(float)))
+                            : nullptr;
+    }
     auto* st = static_cast<unsigned long long*>(
         ws.dev(Workspace::kStats, kStatCount * sizeof(unsigned long long)));
     cuda_check(cudaMemsetAsync(st, 0, kStatCount * sizeof(unsigned long long), s), "memset");
@@ -914,7 +924,8 @@ void exact_search(const ForwardDevice& fwd, const QueryBatch& q, int k, int mode
     cuda_check(cudaEventCreate(&e1), "event");
     cuda_check(cudaEventRecord(e0, s), "event");
     if (fwd.n_docs() > 0) {
-        cuda_check(launch_exact(a, tiles, s), "exact search launch");
+        cuda_check(taat ? launch_exact_taat(a, s) : launch_exact(a, tiles, s),
+                   "exact search launch");
     } else {
         cuda_check(cudaMemsetAsync(dd, 0, cnt * sizeof(float), s), "memset");
     }

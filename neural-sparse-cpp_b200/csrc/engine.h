@@ -149,6 +149,29 @@ private:
     DevArray<uint8_t> val_;
 };
 
+// Doc-ascending postings of an fp32 forward index for the exact search's
+// term-at-a-time path (nsp_device.h, PostingsView), built on the device from
+// the resident rows. Usable only when every row holds strictly ascending
+// terms: then a doc's products, applied term by term, arrive in row order.
+class PostingsDevice {
+public:
+    // (Re)builds from `fwd` for doc chunks of `chunk_docs`.
+    void build(const ForwardDevice& fwd, int chunk_docs);
+    bool usable() const { return usable_; }
+    uint64_t generation() const { return generation_; }  // of the forward index it mirrors
+    PostingsView view() const;
+    size_t device_bytes() const;
+
+private:
+    uint64_t generation_ = 0;
+    bool usable_ = false;
+    int32_t n_chunks_ = 0;
+    int32_t chunk_docs_ = 0;
+    DevArray<int32_t> doc_;
+    DevArray<float> val_;
+    DevArray<int32_t> chunk_at_;
+};
+
 // SEISMIC lists flattened over terms, in host memory (the reference's
 // InvertedListClusters fields per list, cluster/inverted_list_clusters.h:75-84).
 struct SeismicHost {
@@ -271,8 +294,10 @@ void seismic_search(const ForwardDevice& fwd, const SeismicDevice& ix, const Que
                     const SeismicSearchArgs& args, const std::vector<uint64_t>* sel_bits,
                     float* out_d, int32_t* out_l, SearchStats* stats);
 
-void exact_search(const ForwardDevice& fwd, const QueryBatch& q, int k, int mode,
-                  const std::vector<uint64_t>* sel_bits, float* out_d, int32_t* out_l,
+// `post` (may be null): the forward index's postings; the term-at-a-time
+// kernel runs when they are usable and k <= kTaatMaxK, else the tile kernel.
+void exact_search(const ForwardDevice& fwd, const PostingsDevice* post, const QueryBatch& q, int k,
+                  int mode, const std::vector<uint64_t>* sel_bits, float* out_d, int32_t* out_l,
                   SearchStats* stats);
 
 void exact_list_search(const ForwardDevice& fwd, const QueryBatch& q, const SeismicSearchArgs& args,

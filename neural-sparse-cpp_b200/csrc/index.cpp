@@ -208,10 +208,27 @@ void ForwardState::ensure_device() {
     }
 }
 
+const nsp::PostingsDevice* ForwardState::ensure_postings() {
+    std::lock_guard<std::mutex> g(mu);
+    if (dirty) {
+        dev.upload(host);
+        dirty = false;
+    }
+    if (post.generation() != dev.generation()) post.build(dev, nsp::exact_taat_chunk_docs());
+    return &post;
+}
+
 bool ForwardState::terms_in_range(int dim) const {
-    for (uint16_t t : host.indices)
-        if (t >= dim) return false;
-    return true;
+    std::lock_guard<std::mutex> g(mu);
+    const std::vector<uint16_t>& ix = host.indices;
+    if (ix.data() != scanned_at || ix.size() < scanned_len) {
+        scanned_len = 0;
+        max_term = -1;
+    }
+    for (size_t i = scanned_len; i < ix.size(); ++i) max_term = std::max<int>(max_term, ix[i]);
+    scanned_at = ix.data();
+    scanned_len = ix.size();
+    return max_term < dim;
 }
 
 }  // namespace detail
@@ -295,10 +312,10 @@ void BrutalIndex::search_impl(idx_t n, const idx_t* indptr, const term_t* indice
                               SearchParameters*) {
     if (fwd_->host.n() == 0) return fill_padding(n, k, distances, labels);
     if (!fwd_->terms_in_range(dimension_)) throw std::invalid_argument("term_id out of range");
-    fwd_->ensure_device();
+    const nsp::PostingsDevice* post = fwd_->ensure_postings();
     const nsp::QueryBatch q = nsp::canonicalize(n, indptr, indices, values, dimension_);
     nsp::SearchStats st;
-    nsp::exact_search(fwd_->dev, q, k, 0, nullptr, distances, labels, &st);
+    nsp::exact_search(fwd_->dev, post, q, k, 0, nullptr, distances, labels, &st);
     record_stats(st);
 }
 
@@ -327,13 +344,14 @@ void InvertedIndex::search_impl(idx_t n, const idx_t* indptr, const term_t* indi
                                 const float* values, int k, float* distances, idx_t* labels,
                                 SearchParameters* params) {
     if (!built_ || fwd_->host.n() == 0) return fill_padding(n, k, distances, labels);
-    fwd_->ensure_device();
+    const nsp::PostingsDevice* post = fwd_->ensure_postings();
     const nsp::QueryBatch q = nsp::canonicalize(n, indptr, indices, values, dimension_);
     const IDSelector* sel = params == nullptr ? nullptr : params->get_id_selector();
     std::vector<uint64_t> bits;
     if (sel != nullptr) bits = detail::selector_bitmap(sel, fwd_->host.n());
     nsp::SearchStats st;
-    nsp::exact_search(fwd_->dev, q, k, 1, sel != nullptr ? &bits : nullptr, distances, labels, &st);
+    nsp::exact_search(fwd_->dev, post, q, k, 1, sel != nullptr ? &bits : nullptr, distances, labels,
+                      &st);
     record_stats(st);
 }
 

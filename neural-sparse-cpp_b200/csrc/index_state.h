@@ -24,11 +24,21 @@ struct ForwardState {
     }
     nsp::HostCsr host;
     nsp::ForwardDevice dev;
+    nsp::PostingsDevice post;  // exact search's term-at-a-time postings
     bool dirty = true;
-    std::mutex mu;
+    mutable std::mutex mu;
     void append(idx_t n, const idx_t* indptr, const term_t* indices, const uint8_t* value_bytes);
     void ensure_device();
+    // ensure_device, then the postings of the device rows (rebuilt after
+    // every upload).
+    const nsp::PostingsDevice* ensure_postings();
+    // Every stored term < dim. The largest term is kept and extended over
+    // appended elements only (a replaced host array is scanned afresh), so a
+    // search does not rescan the whole index.
     bool terms_in_range(int dim) const;
+    mutable const uint16_t* scanned_at = nullptr;
+    mutable size_t scanned_len = 0;
+    mutable int max_term = -1;
 };
 
 struct SeismicState {

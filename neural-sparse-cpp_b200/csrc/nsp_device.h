@@ -118,8 +118,23 @@ struct SeismicLaunch {
     int32_t cluster;
 };
 
+// Doc-ascending postings of an fp32 forward index (the exact search's
+// term-at-a-time path): term t's postings are doc/val[chunk_at[t * (n_chunks
+// + 1)] .. chunk_at[t * (n_chunks + 1) + n_chunks]), docs ascending, and
+// chunk_at[t * (n_chunks + 1) + c] is the first of them with doc >= c *
+// chunk_docs, so a CTA scoring doc chunk c finds each query term's run with
+// two loads.
+struct PostingsView {
+    int32_t n_chunks;
+    int32_t chunk_docs;
+    const int32_t* doc;
+    const float* val;
+    const int32_t* chunk_at;    // [dim][n_chunks + 1]
+};
+
 struct ExactLaunch {
     FwdView fwd;
+    PostingsView post;          // term-at-a-time path (launch_exact_taat)
     QueryView q;
     int k;
     int mode;                   // 0 brutal (all docs), 1 inverted (score > 0)
@@ -175,6 +190,13 @@ cudaError_t launch_seismic_cta(int val_kind, const SeismicLaunch& a, int warps, 
 
 size_t exact_smem(int dim_words, int qcap_smem);  // qcap_smem 0: values in global
 cudaError_t launch_exact(const ExactLaunch& a, int tiles, cudaStream_t s);
+
+// Term-at-a-time exact search (search_exact_taat.cu): one CTA per (query, doc
+// chunk of a.post), k <= kTaatMaxK; candidates per chunk in a.cand_d/l
+// [n_q][n_chunks][k], then the tile path's merge.
+constexpr int kTaatMaxK = 128;
+int exact_taat_chunk_docs();  // docs per chunk that keep 4 CTAs per SM
+cudaError_t launch_exact_taat(const ExactLaunch& a, cudaStream_t s);
 
 // Exact scoring of an explicit doc list per query (the reference's
 // ExactMatcher, exact_matcher.h:23-58): ids ascending, at most k of them.

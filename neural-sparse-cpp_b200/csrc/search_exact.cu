@@ -15,6 +15,10 @@
 // its docs in ascending id order, so "reject score <= min" resolves ties to
 // the lower id (utils/ranker.h:147-200). The CTA merges its warps' lists per
 // query, and a second kernel merges the tiles.
+//
+// The term-at-a-time kernel below is the default for indexes whose rows hold
+// strictly ascending terms and for k <= kTaatMaxK; the tile kernel serves the
+// rest.
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -293,9 +297,207 @@ __global__ void __launch_bounds__(32) exact_merge_kernel(const float* cand_d, co
     }
 }
 
+// ------------------------------------------------- term at a time --
+// One CTA per (query, doc chunk): the chunk's scores live in shared memory,
+// and the query's terms are applied one after another in ascending term order
+// -- term t adds w * q_t to every doc of the chunk in t's postings, a barrier
+// between terms. A doc's score thus receives its nonzero products in
+// ascending term order, which for a row stored with strictly ascending terms
+// is its row order: the reference's sequential sum (utils/distance.h:29-37)
+// with the zero products of non-query terms left out, and adding +-0 to a sum
+// that starts at +0 changes nothing. The host takes this path only for such
+// rows. Work per query is the postings of its terms (~8% of the index on
+// the reference corpus shape) instead of every row.
+constexpr int kTWarps = 8;
+constexpr int kTermWin = 256;  // query terms whose runs are located at once
+
+__host__ __device__ inline size_t taat_smem_bytes(int chunk_docs, int k) {
+    return static_cast<size_t>(chunk_docs) * 4 + static_cast<size_t>(kTermWin) * 12 +
+           static_cast<size_t>(kTWarps) * k * 8;
+}
+
+__global__ void __launch_bounds__(kTWarps * 32) exact_taat_kernel(ExactLaunch a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const PostingsView& P = a.post;
+    const int nq = a.q.n;
+    const int c = static_cast<int>(blockIdx.x / static_cast<unsigned>(nq));  // chunk-major
+    const int qi = static_cast<int>(blockIdx.x - static_cast<unsigned>(c) * nq);
+    float* sc = reinterpret_cast<float*>(smem);
+    int32_t* tlo = reinterpret_cast<int32_t*>(sc + P.chunk_docs);
+    int32_t* thi = tlo + kTermWin;
+    float* tqv = reinterpret_cast<float*>(thi + kTermWin);
+    float* lsd = tqv + kTermWin;
+    int32_t* lsi = reinterpret_cast<int32_t*>(lsd + kTWarps * a.k);
+
+    const int32_t d0 = c * P.chunk_docs;
+    const int nd = min(P.chunk_docs, a.fwd.n_docs - d0);
+    for (int i = threadIdx.x; i < nd; i += blockDim.x) sc[i] = 0.0f;
+    const int32_t qs = a.q.indptr[qi];
+    const int qn = a.q.indptr[qi + 1] - qs;
+    const uint16_t* qt = a.q.idx + qs;
+    const float* qv = static_cast<const float*>(a.q.val) + qs;
+    const int stride = P.n_chunks + 1;
+    const int B = blockDim.x;
+    unsigned long long postings = 0;
+    for (int w0 = 0; w0 < qn; w0 += kTermWin) {
+        const int wn = min(kTermWin, qn - w0);
+        __syncthreads();  // zeroing, or the previous window's runs, done
+        for (int i = threadIdx.x; i < wn; i += B) {
+            const size_t row = static_cast<size_t>(qt[w0 + i]) * stride + c;
+            tlo[i] = __ldg(P.chunk_at + row);
+            thi[i] = __ldg(P.chunk_at + row + 1);
+            tqv[i] = qv[w0 + i];
+        }
+        __syncthreads();
+        for (int i = 0; i < wn; ++i) {
+            const int32_t lo = tlo[i];
+            const int32_t hi = thi[i];
+            const float q = tqv[i];
+            postings += static_cast<unsigned long long>(hi - lo);
+            int32_t p = lo + static_cast<int32_t>(threadIdx.x);
+            // four postings' loads in flight before their updates; a term's
+            // docs are distinct, so the updates of one term never collide
+            for (; p + 3 * B < hi; p += 4 * B) {
+                int32_t d[4];
+                float w[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    d[u] = __ldg(P.doc + p + u * B);
+                    w[u] = __ldg(P.val + p + u * B);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    float* s = sc + (d[u] - d0);
+                    *s = __fadd_rn(*s, __fmul_rn(w[u], q));
+                }
+            }
+            for (; p < hi; p += B) {
+                float* s = sc + (__ldg(P.doc + p) - d0);
+                *s = __fadd_rn(*s, __fmul_rn(__ldg(P.val + p), q));
+            }
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+
+    // Top-k of the chunk: warp w keeps a sorted list of its contiguous docs,
+    // visited in ascending id order, so "reject score <= min" once full
+    // resolves ties to the lower id (utils/ranker.h:147-200).
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int per = (nd + kTWarps - 1) / kTWarps;
+    const int lo = warp * per;
+    const int hi = min(nd, lo + per);
+    float* ls = lsd + warp * a.k;
+    int32_t* li = lsi + warp * a.k;
+    int n = 0;
+    float thr = -FLT_MAX;
+    for (int b = lo; b < hi; b += 32) {
+        const int i = b + lane;
+        bool ok = i < hi;
+        const float s = ok ? sc[i] : 0.0f;
+        const int32_t d = d0 + i;
+        if (ok && a.mode == 1) {
+            if (!(s > 0.0f)) ok = false;
+            if (a.sel_bits != nullptr && !((__ldg(a.sel_bits + (d >> 6)) >> (d & 63)) & 1ull))
+                ok = false;
+        }
+        unsigned m = __ballot_sync(kFull, ok && (n < a.k || s > thr));
+        while (m != 0u) {
+            const int L = __ffs(m) - 1;
+            m &= m - 1u;
+            const float sL = __shfl_sync(kFull, s, L);
+            if (n == a.k && !(sL > thr)) continue;  // the list moved on
+            if (lane == 0) {
+                int nn = n;
+                list_insert(ls, li, nn, a.k, sL, d0 + b + L);
+            }
+            if (n < a.k) ++n;
+            __syncwarp();
+            if (n == a.k) thr = ls[a.k - 1];
+        }
+    }
+    for (int i = n + lane; i < a.k; i += 32) {
+        ls[i] = -FLT_MAX;
+        li[i] = INT_MAX;
+    }
+    if (a.stats != nullptr && threadIdx.x == 0)
+        atomicAdd(a.stats + kStatBytes, postings * 8ull + static_cast<unsigned long long>(qn) * 8ull);
+    __syncthreads();
+
+    // Merge the warps' lists into the chunk's candidates: lane w < kTWarps
+    // holds list w's head; lane 0's choice is the warp's.
+    if (warp == 0) {
+        int head = 0;
+        float* cd = a.cand_d + (static_cast<size_t>(qi) * P.n_chunks + c) * a.k;
+        int32_t* cl = a.cand_l + (static_cast<size_t>(qi) * P.n_chunks + c) * a.k;
+        for (int r = 0; r < a.k; ++r) {
+            float bs = -FLT_MAX;
+            int32_t bi = INT_MAX;
+            int bl = -1;
+            if (lane < kTWarps && head < a.k) {
+                const int32_t id = lsi[lane * a.k + head];
+                if (id != INT_MAX) {
+                    bs = lsd[lane * a.k + head];
+                    bi = id;
+                    bl = lane;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const float s2 = __shfl_xor_sync(kFull, bs, o);
+                const int32_t i2 = __shfl_xor_sync(kFull, bi, o);
+                const int l2 = __shfl_xor_sync(kFull, bl, o);
+                if (l2 >= 0 && (bl < 0 || better(s2, i2, bs, bi))) {
+                    bs = s2;
+                    bi = i2;
+                    bl = l2;
+                }
+            }
+            bl = __shfl_sync(kFull, bl, 0);
+            bs = __shfl_sync(kFull, bs, 0);
+            bi = __shfl_sync(kFull, bi, 0);
+            if (lane == 0) {
+                cd[r] = bl < 0 ? -FLT_MAX : bs;
+                cl[r] = bl < 0 ? INT_MAX : bi;
+            }
+            if (lane == bl) ++head;
+        }
+    }
+}
+
 }  // namespace
 
 size_t exact_smem(int dim_words, int qcap_smem) { return exact_smem_bytes(dim_words, qcap_smem); }
+
+int exact_taat_chunk_docs() {
+    int dev = 0;
+    int per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) !=
+            cudaSuccess)
+        per_sm = 228 * 1024;
+    // four CTAs per SM (1 KB of each CTA's share is reserved by the device)
+    const long long room = per_sm / 4 - 1024 - static_cast<long long>(taat_smem_bytes(0, kTaatMaxK));
+    const long long docs = (room / 4) & ~255ll;
+    return static_cast<int>(docs < 1024 ? 1024 : docs);
+}
+
+cudaError_t launch_exact_taat(const ExactLaunch& a, cudaStream_t s) {
+    if (a.q.n == 0) return cudaSuccess;
+    if (a.k > kTaatMaxK) return cudaErrorInvalidValue;
+    const size_t smem = taat_smem_bytes(a.post.chunk_docs, a.k);
+    cudaError_t e = allow_opt_in_smem(exact_taat_kernel);
+    if (e != cudaSuccess) return e;
+    const long long grid = static_cast<long long>(a.post.n_chunks) * a.q.n;
+    if (grid > 0x7fffffffll) return cudaErrorInvalidValue;
+    exact_taat_kernel<<<static_cast<unsigned>(grid), kTWarps * 32, smem, s>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    exact_merge_kernel<<<a.q.n, 32, static_cast<size_t>(a.post.n_chunks) * sizeof(int), s>>>(
+        a.cand_d, a.cand_l, a.post.n_chunks, a.k, a.out_d, a.out_l);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_exact(const ExactLaunch& a, int tiles, cudaStream_t s) {
     if (a.q.n == 0) return cudaSuccess;

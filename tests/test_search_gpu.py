@@ -93,6 +93,87 @@ def test_exact_paths_match_oracle_medium(k):
     np.testing.assert_array_equal(D, Do)
 
 
+def _unsorted_rows(docs, seed):
+    """The same docs with every row's elements in a random order, and a
+    repeated term (at a new value) appended to every tenth row: rows that
+    are not strictly ascending, summed by the reference in stored order."""
+    rng = np.random.default_rng(seed)
+    ip, ix, vv = [0], [], []
+    for d in range(docs.n):
+        s, e = int(docs.indptr[d]), int(docs.indptr[d + 1])
+        perm = rng.permutation(e - s)
+        t, v = docs.indices[s:e][perm], docs.values[s:e][perm]
+        if d % 10 == 0 and e > s:
+            t = np.append(t, t[0])
+            v = np.append(v, np.float32(rng.lognormal(0.0, 0.8)))
+        ix.append(t)
+        vv.append(v)
+        ip.append(ip[-1] + len(t))
+    return synth.Csr(docs.dim, np.array(ip, np.int32), np.concatenate(ix).astype(np.uint16),
+                     np.concatenate(vv).astype(np.float32))
+
+
+@pytest.mark.parametrize("k", [10, 200])
+def test_exact_paths_unsorted_rows_and_large_k(k):
+    """Term-at-a-time scoring needs strictly ascending rows and k <= 128; an
+    index with unsorted or repeated terms, or a larger k, takes the tile kernel.
+    Every combination equals the oracle bit for bit."""
+    base = synth.docs_config0(20000, seed=8)
+    qs = synth.queries_config0(100, seed=8)
+    for docs in (base, _unsorted_rows(base, 9)):
+        b = make("brutal", docs, build=False)
+        D, L = search(b, qs, k)
+        Do, Lo = O.exact_search(docs, qs, k, 0)
+        np.testing.assert_array_equal(L, Lo)
+        np.testing.assert_array_equal(D, Do)
+        v = make("inverted", docs)
+        D, L = search(v, qs, k)
+        Do, Lo = O.exact_search(docs, qs, k, 1)
+        np.testing.assert_array_equal(L, Lo)
+        np.testing.assert_array_equal(D, Do)
+
+
+def test_exact_paths_selector_empty_queries_and_readd():
+    """Across several doc chunks: a 10% selector on the inverted index, empty
+    query rows (brutal: the first k docs at score 0; inverted: padding), and a
+    second add(), after which the postings follow the grown index."""
+    docs = synth.docs_config0(40000, seed=11)
+    qs = synth.queries_config0(80, seed=11)
+    ip = qs.indptr.copy()
+    keep = np.ones(qs.nnz, bool)
+    for q in (3, 40):  # empty rows 3 and 40
+        keep[ip[q]:ip[q + 1]] = False
+    lens = np.diff(ip)
+    lens[[3, 40]] = 0
+    qe = synth.Csr(qs.dim, np.concatenate([[0], np.cumsum(lens)]).astype(np.int32),
+                   qs.indices[keep], qs.values[keep])
+    rng = np.random.default_rng(12)
+    ids = np.sort(rng.choice(docs.n, docs.n // 10, replace=False)).astype(np.int32)
+    v = make("inverted", docs)
+    p = nsparse.SearchParameters()
+    p.set_id_selector(nsparse.SetIDSelector(ids))
+    D, L = search(v, qe, 10, p)
+    Do, Lo = O.exact_search(docs, qe, 10, 1, sel_bits=O.bitmap_from_ids(docs.n, ids))
+    np.testing.assert_array_equal(L, Lo)
+    np.testing.assert_array_equal(D, Do)
+    assert (L[[3, 40]] == -1).all()
+    b = make("brutal", docs, build=False)
+    D, L = search(b, qe, 10)
+    Do, Lo = O.exact_search(docs, qe, 10, 0)
+    np.testing.assert_array_equal(L, Lo)
+    np.testing.assert_array_equal(D, Do)
+    np.testing.assert_array_equal(L[3], np.arange(10))
+    more = synth.docs_config0(15000, seed=13)
+    b.add(more.n, more.indptr, more.indices, more.values)
+    grown = synth.Csr(docs.dim, np.concatenate([docs.indptr, more.indptr[1:] + docs.nnz]).astype(np.int32),
+                      np.concatenate([docs.indices, more.indices]),
+                      np.concatenate([docs.values, more.values]))
+    D, L = search(b, qs, 10)
+    Do, Lo = O.exact_search(grown, qs, 10, 0)
+    np.testing.assert_array_equal(L, Lo)
+    np.testing.assert_array_equal(D, Do)
+
+
 def test_brutal_ignores_selector_and_pads():
     docs, qs = golden_corpus()
     idx = make("brutal", docs, build=False)
