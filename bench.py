@@ -696,6 +696,76 @@ def run_engine_brutal(args):
         "cpu_baseline": cpu}))
 
 
+def _sha256(path):
+    import hashlib
+    h = hashlib.sha256()
+    with open(path, "rb") as f:
+        for chunk in iter(lambda: f.read(1 << 24), b""):
+            h.update(chunk)
+    return h.hexdigest()
+
+
+def run_engine_build(args):
+    """SEISMIC build of the benchmark index (1M docs, lambda=4000, beta=400,
+    alpha=0.4, seed 7) on the device, beside the reference's own build with
+    its cuSPARSE GPU offload (oracle/_ref/libnsparse_ref_avx512_gpu.so, the
+    reference's stock settings: assignment on the GPU, summaries on the CPU,
+    all host threads), on the same corpus and box. The two index files are
+    compared list by list."""
+    import filecmp
+    import torch
+    torch.cuda.set_device(0)
+    import nsparse
+    import oracle as O
+    docs, _ = make_data(0)
+    out = tempfile.mkdtemp()
+    ours_path, ref_path = os.path.join(out, "ours.idx"), os.path.join(out, "ref_gpu.idx")
+    times = []
+    for _ in range(max(args.steps, 1)):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        idx = nsparse.index_factory(docs.dim, SPEC)
+        idx.add(docs.n, docs.indptr, docs.indices, docs.values)
+        idx.build()
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t)
+    nsparse.write_index(idx, ours_path)
+    del idx
+    ref = None
+    if O.ref_available("avx512_gpu") and not args.no_cpu:
+        cores = os.cpu_count()
+        O.ref_lib("avx512_gpu").ref_set_threads(cores)
+        t = time.perf_counter()
+        r = O.RefIndex(docs.dim, SPEC, variant="avx512_gpu")
+        r.add(docs)
+        r.build()
+        ref_s = time.perf_counter() - t
+        r.write(ref_path)
+        r.close()
+        same = filecmp.cmp(ours_path, ref_path, shallow=False)
+        lists_same = 1.0
+        if not same:
+            a, b = O.read_index_file(ours_path)["lists"], O.read_index_file(ref_path)["lists"]
+            eq = [np.array_equal(x["docs"], y["docs"]) and np.array_equal(x["offsets"], y["offsets"])
+                  for x, y in zip(a, b)]
+            lists_same = float(np.mean(eq)) if eq else 1.0
+        ref = {"seconds": ref_s, "threads": cores,
+               "kind": "reference, cuSPARSE GPU offload (nsparse/gpu), AVX-512 host code",
+               "index_files_identical": bool(same), "lists_identical_frac": lists_same,
+               "sha256": _sha256(ref_path)}
+        log(f"reference GPU-offload build {ref_s:.1f}s on {cores} threads; identical={same}")
+    value = statistics.median(times)
+    print(json.dumps({
+        "metric": "SEISMIC build seconds (fp32, 1M docs)", "value": value, "unit": "s",
+        "n_gpus": 1, "steps": len(times), "warmup": 0, "ms_per_step": 1000 * value,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"seismic_build_fp32_{docs.n}_docs", "lambda": 4000, "beta": 400,
+                   "alpha": 0.4, "seed": 7},
+        "build_s_each": times, "index_sha256": _sha256(ours_path), "reference_gpu_offload": ref,
+        "speedup_vs_reference_gpu_offload": None if ref is None else ref["seconds"] / value}))
+
+
 def serve_sweep(nsparse, idx, docs, qs, cut, hf, rates, seconds=2.0, slots=3):
     """Serving loop under Poisson arrivals: per offered rate, ~`seconds` of
     requests (k 10 or 100 at random, 30% carrying a doc filter that admits a
@@ -759,11 +829,13 @@ def main():
     ap.add_argument("--serve-rates", default="5000,20000,50000,100000,200000",
                     type=lambda s: [float(x) for x in s.split(",") if x],
                     help="offered request rates (queries/s) for the serving sweep")
-    ap.add_argument("--workload", default="fp32-1m", choices=["fp32-1m", "sq8-8.8m", "brutal-100k"],
+    ap.add_argument("--workload", default="fp32-1m",
+                    choices=["fp32-1m", "sq8-8.8m", "brutal-100k", "build-1m"],
                     help="fp32-1m: the headline workload; sq8-8.8m: SEISMIC-SQ at 8.8M docs "
-                         "with the serving sweep; brutal-100k: exact brute force")
+                         "with the serving sweep; brutal-100k: exact brute force; build-1m: "
+                         "the device build beside the reference's GPU-offload build")
     args = ap.parse_args()
-    if args.workload == "fp32-1m" and (args.docs or args.queries):
+    if args.workload in ("fp32-1m", "build-1m") and (args.docs or args.queries):
         N_DOCS, N_QUERIES = args.docs or N_DOCS, args.queries or N_QUERIES
         WORKLOAD.update(workload=f"seismic_fp32_{N_DOCS}_docs_{N_QUERIES}_queries", docs=N_DOCS,
                         queries=N_QUERIES)
@@ -771,6 +843,8 @@ def main():
         run_engine_sq(args)
     elif args.workload == "brutal-100k":
         run_engine_brutal(args)
+    elif args.workload == "build-1m":
+        run_engine_build(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
