@@ -696,6 +696,27 @@ def run_engine_brutal(args):
         "cpu_baseline": cpu}))
 
 
+def list_digests(path):
+    """One line per posting list of an index file: a digest of its blocks
+    (n_clusters, offsets, docs) and one of its summaries (term_ids, term_ptr,
+    csc_cluster, csc_value)."""
+    import hashlib
+    import oracle as O
+    rows = []
+    for c in O.read_index_file(path)["lists"]:
+        parts = []
+        for keys in (("n_clusters", "offsets", "docs"),
+                     ("term_ids", "term_ptr", "csc_cluster", "csc_value")):
+            h = hashlib.sha256()
+            for key in keys:
+                v = c[key]
+                h.update(np.ascontiguousarray(v).tobytes() if isinstance(v, np.ndarray)
+                         else repr(int(v)).encode())
+            parts.append(h.hexdigest()[:16])
+        rows.append(" ".join(parts))
+    return rows
+
+
 def _sha256(path):
     import hashlib
     h = hashlib.sha256()
@@ -731,6 +752,12 @@ def run_engine_build(args):
         times.append(time.perf_counter() - t)
     nsparse.write_index(idx, ours_path)
     del idx
+    if args.digest_out:
+        # per posting list, short digests of its blocks (docs, offsets) and of
+        # its summaries, to compare with a reference file built elsewhere
+        # from the same corpus
+        with open(args.digest_out, "w") as f:
+            f.write("\n".join(list_digests(ours_path)))
     ref = None
     if O.ref_available("avx512_gpu") and not args.no_cpu:
         cores = os.cpu_count()
@@ -829,6 +856,8 @@ def main():
     ap.add_argument("--serve-rates", default="5000,20000,50000,100000,200000",
                     type=lambda s: [float(x) for x in s.split(",") if x],
                     help="offered request rates (queries/s) for the serving sweep")
+    ap.add_argument("--digest-out", default="",
+                    help="build-1m: write one digest per posting list of the device-built file")
     ap.add_argument("--workload", default="fp32-1m",
                     choices=["fp32-1m", "sq8-8.8m", "brutal-100k", "build-1m"],
                     help="fp32-1m: the headline workload; sq8-8.8m: SEISMIC-SQ at 8.8M docs "

@@ -74,7 +74,9 @@ def build_engine(force=False, jobs=8):
         obj = os.path.join(OBJ, os.path.basename(src) + ".o")
         objs.append(obj)
         if force or _stale(obj, [src] + hdrs):
-            tasks.append([cxx, "-O3", "-std=c++17", "-fPIC", "-Wall", "-Wno-unused-function",
+            # ref_order.cpp makes the reference's C++20 library calls
+            std = "-std=c++20" if os.path.basename(src) == "ref_order.cpp" else "-std=c++17"
+            tasks.append([cxx, "-O3", std, "-fPIC", "-Wall", "-Wno-unused-function",
                           f"-I{CUDA}/include", *INCLUDES, "-c", src, "-o", obj])
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
         list(ex.map(_run, tasks))

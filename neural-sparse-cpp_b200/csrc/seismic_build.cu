@@ -47,6 +47,7 @@
 
 #include "engine.h"
 #include "index_state.h"
+#include "ref_order.h"
 #include "scan.h"
 
 namespace nsparse {
@@ -171,6 +172,26 @@ __global__ void kept_copy_kernel(const uint64_t* keys, const int64_t* post_ptr,
         const int64_t n = kept_ptr[t + 1] - kept_ptr[t];
         for (int64_t i = threadIdx.x; i < n; i += blockDim.x)
             kept[kept_ptr[t] + i] = static_cast<int32_t>(keys[post_ptr[t] + i] & 0xffffffffu);
+    }
+}
+
+// Flags a truncated list (len > cap) whose first cap + 1 sorted keys hold two
+// equal values: its kept order (and, with a tie across the cut, its kept set)
+// is what the reference's unstable sort leaves, which the host reproduces.
+__global__ void tie_flag_kernel(const uint64_t* keys, const int64_t* post_ptr, int32_t n_lists,
+                                int64_t cap, uint8_t* flag) {
+    for (int32_t t = blockIdx.x; t < n_lists; t += gridDim.x) {
+        const int64_t len = post_ptr[t + 1] - post_ptr[t];
+        if (cap <= 0 || len <= cap) {
+            if (threadIdx.x == 0) flag[t] = 0;
+            continue;
+        }
+        const uint64_t* k = keys + post_ptr[t];
+        int tie = 0;
+        for (int64_t i = threadIdx.x + 1; i <= cap; i += blockDim.x)
+            tie |= (k[i] >> 32) == (k[i - 1] >> 32);
+        tie = __syncthreads_or(tie);
+        if (threadIdx.x == 0) flag[t] = static_cast<uint8_t>(tie);
     }
 }
 
@@ -879,6 +900,26 @@ void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
     g_steps.mark("columns");
 }
 
+// fp32 lists whose kept postings hold tied values get the reference's kept
+// order from the host (ref_order.cpp); every other list's device order
+// (value desc, then doc asc) is already the reference's.
+void reference_tie_order(const nsp::HostCsr& h, const std::vector<int64_t>& post,
+                         const std::vector<int64_t>& kept_ptr, const std::vector<uint8_t>& tie,
+                         int64_t cap, DevArray<int32_t>& kept, cudaStream_t s) {
+    std::vector<int32_t> lists;
+    for (int32_t t = 0; t < static_cast<int32_t>(tie.size()); ++t)
+        if (tie[t]) lists.push_back(t);
+    if (lists.empty()) return;
+    std::vector<int32_t> out;
+    nsp::reference_kept_order(h, post, lists, cap, out);
+    for (size_t j = 0; j < lists.size(); ++j)
+        cuda_check(cudaMemcpyAsync(kept.data() + kept_ptr[lists[j]], out.data() + j * cap,
+                                   static_cast<size_t>(cap) * sizeof(int32_t),
+                                   cudaMemcpyHostToDevice, s),
+                   "H2D kept order");
+    cuda_check(cudaStreamSynchronize(s), "sync");
+}
+
 // Phase timings on stderr when NSP_VERBOSE=1 (the engine's one debug switch).
 struct PhaseClock {
     cudaStream_t s;
@@ -950,8 +991,17 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
     kept_copy_kernel<<<sms * 8, 256, 0, s>>>(keys2.data(), post_ptr.data(), d_kept_ptr.data(),
                                              n_lists, kept.data());
     cuda_check(cudaGetLastError(), "kept_copy_kernel");
+    std::vector<uint8_t> tie(static_cast<size_t>(n_lists), 0);
+    if (ESZ == 4 && cap > 0) {
+        DevArray<uint8_t> d_tie(static_cast<size_t>(n_lists));
+        tie_flag_kernel<<<sms * 8, 256, 0, s>>>(keys2.data(), post_ptr.data(), n_lists, cap,
+                                                d_tie.data());
+        cuda_check(cudaGetLastError(), "tie_flag_kernel");
+        d_tie.download(tie.data(), tie.size(), s);
+    }
     cuda_check(cudaStreamSynchronize(s), "sync");
     keys2.reset();
+    if (ESZ == 4) reference_tie_order(h, h_post, kept_ptr, tie, cap, kept, s);
 
     clock.mark("postings");
     // ---- 2. centroid positions (host; depends on list lengths only)
