@@ -769,6 +769,9 @@ def run_engine_build(args):
         ref_s = time.perf_counter() - t
         r.write(ref_path)
         r.close()
+        if args.digest_out:
+            with open(args.digest_out + ".reference_gpu", "w") as f:
+                f.write("\n".join(list_digests(ref_path)))
         same = filecmp.cmp(ours_path, ref_path, shallow=False)
         lists_same = 1.0
         if not same:
