@@ -331,10 +331,12 @@ void InvertedIndex::add(idx_t n, const idx_t* indptr, const term_t* indices,
     fwd_->append(n, indptr, indices, reinterpret_cast<const uint8_t*>(values));
 }
 
-// inverted_index.cpp:236-252: a term >= dimension has no posting list.
+// inverted_index.cpp:236-252: a term >= dimension has no posting list. The
+// device postings of the exact search are built here, as the reference
+// builds its posting lists here.
 void InvertedIndex::build() {
     if (!fwd_->terms_in_range(dimension_)) throw std::invalid_argument("term_id out of range");
-    fwd_->ensure_device();
+    fwd_->ensure_postings();
     built_ = true;
 }
 
