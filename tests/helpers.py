@@ -107,3 +107,23 @@ def sq_exact_scores(docs, q_codes, qs, labels, vmin, vmax):
             a, b = docs.indptr[d], docs.indptr[d + 1]
             out[q, j] = np.float32(int(np.dot(d_codes[a:b].astype(np.int64), qd[docs.indices[a:b]])))
     return out
+
+
+def unsorted_rows(docs, seed):
+    """The same docs with every row's elements in a random order, and a
+    repeated term (at a new value) appended to every tenth row: rows that
+    are not strictly ascending, summed by the reference in stored order."""
+    rng = np.random.default_rng(seed)
+    ip, ix, vv = [0], [], []
+    for d in range(docs.n):
+        s, e = int(docs.indptr[d]), int(docs.indptr[d + 1])
+        perm = rng.permutation(e - s)
+        t, v = docs.indices[s:e][perm], docs.values[s:e][perm]
+        if d % 10 == 0 and e > s:
+            t = np.append(t, t[0])
+            v = np.append(v, np.float32(rng.lognormal(0.0, 0.8)))
+        ix.append(t)
+        vv.append(v)
+        ip.append(ip[-1] + len(t))
+    return synth.Csr(docs.dim, np.array(ip, np.int32), np.concatenate(ix).astype(np.uint16),
+                     np.concatenate(vv).astype(np.float32))

@@ -9,7 +9,8 @@ import pytest
 import oracle as O
 from helpers import CUT, HF, K, SEISMIC, golden, golden_corpus, oracle_seismic_from_file, \
     sq_exact_scores, \
-    recall, ref_file, ref_index, sq_spec
+    recall, ref_file, ref_index, sq_spec, unsorted_rows
+from nsparse_b200 import synth
 
 need_ref = pytest.mark.skipif(not O.ref_available(), reason="reference library not built")
 
@@ -57,6 +58,23 @@ def test_dot_product_known_answers():
 
 
 # --- golden results of the reference ---------------------------------------
+
+@need_ref
+def test_exact_oracle_matches_reference_on_unsorted_rows():
+    """Rows stored out of term order, some repeating a term: the reference's
+    BrutalIndex sums each row in stored order (utils/distance.h:29-37), and so
+    does the oracle, bit for bit. The GPU tests compare both exact kernels
+    with the oracle on these rows."""
+    docs = unsorted_rows(synth.docs_config0(3000, seed=8), 9)
+    qs = synth.queries_config0(60, seed=8)
+    r = O.RefIndex(docs.dim, "brutal", variant="generic")
+    r.add(docs)
+    Dr, Lr = r.search(qs, 37)
+    r.close()
+    D, L = O.exact_search(docs, qs, 37, 0)
+    np.testing.assert_array_equal(L, Lr)
+    np.testing.assert_array_equal(D, Dr)
+
 
 def test_exact_oracle_matches_reference_golden():
     g = golden()

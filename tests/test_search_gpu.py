@@ -13,7 +13,7 @@ import pytest
 import nsparse
 import oracle as O
 from helpers import CUT, HF, K, SEISMIC, golden, golden_corpus, oracle_seismic_from_file, recall, \
-    ref_file, sq_exact_scores, sq_spec
+    ref_file, sq_exact_scores, sq_spec, unsorted_rows
 from nsparse_b200 import synth
 
 pytestmark = pytest.mark.gpu
@@ -93,26 +93,6 @@ def test_exact_paths_match_oracle_medium(k):
     np.testing.assert_array_equal(D, Do)
 
 
-def _unsorted_rows(docs, seed):
-    """The same docs with every row's elements in a random order, and a
-    repeated term (at a new value) appended to every tenth row: rows that
-    are not strictly ascending, summed by the reference in stored order."""
-    rng = np.random.default_rng(seed)
-    ip, ix, vv = [0], [], []
-    for d in range(docs.n):
-        s, e = int(docs.indptr[d]), int(docs.indptr[d + 1])
-        perm = rng.permutation(e - s)
-        t, v = docs.indices[s:e][perm], docs.values[s:e][perm]
-        if d % 10 == 0 and e > s:
-            t = np.append(t, t[0])
-            v = np.append(v, np.float32(rng.lognormal(0.0, 0.8)))
-        ix.append(t)
-        vv.append(v)
-        ip.append(ip[-1] + len(t))
-    return synth.Csr(docs.dim, np.array(ip, np.int32), np.concatenate(ix).astype(np.uint16),
-                     np.concatenate(vv).astype(np.float32))
-
-
 @pytest.mark.parametrize("k", [10, 200])
 def test_exact_paths_unsorted_rows_and_large_k(k):
     """Term-at-a-time scoring needs strictly ascending rows and k <= 128; an
@@ -120,7 +100,7 @@ def test_exact_paths_unsorted_rows_and_large_k(k):
     Every combination equals the oracle bit for bit."""
     base = synth.docs_config0(20000, seed=8)
     qs = synth.queries_config0(100, seed=8)
-    for docs in (base, _unsorted_rows(base, 9)):
+    for docs in (base, unsorted_rows(base, 9)):
         b = make("brutal", docs, build=False)
         D, L = search(b, qs, k)
         Do, Lo = O.exact_search(docs, qs, k, 0)
