@@ -50,6 +50,10 @@ public:
     void add(idx_t n, const idx_t* indptr, const term_t* indices, const float* values) override;
     void build() override;
     size_t num_vectors() const override;
+    // MmapIndex::read_csr (mmap_index.h:24-36): Residency::kMmap reads the
+    // native layout (nsparse/utils/csr_layout.h), into an index that holds no
+    // vectors yet; kInMemory the interchange layout (Index::read_csr).
+    void read_csr(const char* file_path, Residency residency = Residency::kInMemory) override;
 
     void write_index(IOWriter* writer);
     void read_index(IOReader* reader, int io_flags = 0);

@@ -81,8 +81,16 @@ nsp_status_t nsp_index_dimension(const nsp_index_t* index, int32_t* out);
 nsp_status_t nsp_index_fourcc(const nsp_index_t* index, char out[4]);
 
 /* Index::read_csr (nsparse/index.h:56-58, index.cpp:63-142). residency:
- * 0 in-memory, 1 mmap (accepted; the index is copied to the GPU either way). */
+ * 0 in-memory: the interchange CSR layout; 1 mmap: for a seismic index the
+ * native layout (MmapIndex::read_csr, mmap_index.h:24-36, 72-131; the engine
+ * copies it to the GPU), rejected by a quantized index
+ * (seismic_scalar_quantized_index.cpp:149-157), the interchange layout for
+ * the other index types. */
 nsp_status_t nsp_index_read_csr(nsp_index_t* index, const char* path, int residency);
+
+/* csr_layout::convert (nsparse/utils/csr_layout.h:62-65, csr_layout.cpp:69-156):
+ * rewrites an interchange CSR file in the native layout. */
+nsp_status_t nsp_csr_convert(const char* interchange_path, const char* native_path);
 
 /* write_index / read_index (nsparse/io/index_io.h:29-32). io_flags: 1 =
  * kUseMmap (accepted). The file layout is the reference's. */

@@ -18,6 +18,7 @@
 #include "nsparse/io/index_io.h"
 #include "nsparse/seismic_index.h"
 #include "nsparse/seismic_scalar_quantized_index.h"
+#include "nsparse/utils/csr_layout.h"
 #include "nsparse_c.h"
 
 using namespace nsparse;
@@ -139,6 +140,14 @@ nsp_status_t nsp_index_fourcc(const nsp_index_t* index, char out[4]) {
 nsp_status_t nsp_index_read_csr(nsp_index_t* index, const char* path, int residency) {
     return guarded([&] {
         as_index(index)->read_csr(path, residency == 1 ? Residency::kMmap : Residency::kInMemory);
+    });
+}
+
+nsp_status_t nsp_csr_convert(const char* interchange_path, const char* native_path) {
+    return guarded([&] {
+        if (interchange_path == nullptr || native_path == nullptr)
+            throw std::invalid_argument("unexpected nullptr");
+        nsparse::csr_layout::convert(interchange_path, native_path);
     });
 }
 

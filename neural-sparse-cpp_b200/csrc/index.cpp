@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "csr_layout_read.h"
 #include "index_state.h"
 #include "nsparse/brutal_index.h"
 #include "nsparse/id_map_index.h"
@@ -433,6 +434,16 @@ void SeismicIndex::add(idx_t n, const idx_t* indptr, const term_t* indices, cons
 }
 
 size_t SeismicIndex::num_vectors() const { return static_cast<size_t>(st_->vectors.host.n()); }
+
+void SeismicIndex::read_csr(const char* file_path, Residency residency) {
+    if (residency == Residency::kInMemory) return Index::read_csr(file_path, residency);
+    if (residency != Residency::kMmap) throw std::invalid_argument("invalid residency");
+    if (file_path == nullptr) throw std::invalid_argument("file_path must not be null");
+    if (st_->vectors.host.n() > 0) throw std::runtime_error("mmap index already has vectors");
+    const detail::NativeCsr c = detail::read_native_csr(file_path, dimension_);
+    st_->vectors.append(c.rows, c.indptr.data(), c.indices.data(),
+                        reinterpret_cast<const uint8_t*>(c.values.data()));
+}
 
 void SeismicIndex::build() {
     detail::seismic_build(*st_, dimension_, cluster_parameter_);

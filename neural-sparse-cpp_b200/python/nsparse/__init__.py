@@ -56,6 +56,7 @@ _sig("nsp_index_num_vectors", _P, ctypes.POINTER(ctypes.c_int64))
 _sig("nsp_index_dimension", _P, ctypes.POINTER(_I32))
 _sig("nsp_index_fourcc", _P, ctypes.c_char_p)
 _sig("nsp_index_read_csr", _P, ctypes.c_char_p, ctypes.c_int)
+_sig("nsp_csr_convert", ctypes.c_char_p, ctypes.c_char_p)
 _sig("nsp_write_index", _P, ctypes.c_char_p)
 _sig("nsp_read_index", ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(_P))
 _sig("nsp_id_selector_set_new", ctypes.c_size_t, _P, ctypes.POINTER(_P))
@@ -91,6 +92,45 @@ _sig("nsp_last_search_stats", ctypes.POINTER(_Stats))
 _ERRORS = {1: ValueError, 2: RuntimeError, 3: IndexError, 4: MemoryError}
 
 kUseMmap = 1
+
+# Residency of Index.read_csr (nsparse/types.h), under the names the
+# reference's SWIG module gives the scoped enum.
+Residency_kInMemory = 0
+Residency_kMmap = 1
+
+# CSR file layouts (nsparse/utils/csr_layout.h), flattened into the module
+# as the reference's SWIG interface flattens them.
+kHeaderBytes = 24
+kNativeSuffix = ".mcsr"
+
+
+def padding(pos):
+    """Zero bytes that bring file position `pos` to a 4-byte boundary."""
+    return (4 - pos % 4) % 4
+
+
+def interchange_file_size(indptr_size, nnz):
+    return kHeaderBytes + 8 * indptr_size + 8 * nnz
+
+
+def native_values_offset(indptr_size, nnz):
+    head = kHeaderBytes + 4 * indptr_size + 2 * nnz
+    return head + padding(head)
+
+
+def native_file_size(indptr_size, nnz):
+    return native_values_offset(indptr_size, nnz) + 4 * nnz
+
+
+def native_path(path):
+    return str(path) + kNativeSuffix
+
+
+def convert(interchange_path, native_path):
+    """Rewrites an interchange CSR file (scipy's int64 indptr / int32 indices
+    / float values) in the native layout that read_csr(path,
+    Residency_kMmap) takes."""
+    _check(_L.nsp_csr_convert(str(interchange_path).encode(), str(native_path).encode()))
 
 
 def _check(rc):

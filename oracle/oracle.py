@@ -163,6 +163,8 @@ def ref_lib(variant: str = "generic"):
                                  ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                  ctypes.c_float, ctypes.c_int, I64, P]
         L.ref_write_index.argtypes = [P, ctypes.c_char_p]
+        L.ref_read_csr.argtypes = [P, ctypes.c_char_p, ctypes.c_int]
+        L.ref_csr_convert.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
         L.ref_read_index.restype = P
         L.ref_read_index.argtypes = [ctypes.c_char_p, ctypes.c_int]
         L.ref_set_threads.argtypes = [ctypes.c_int]
@@ -186,6 +188,13 @@ def ref_lib(variant: str = "generic"):
 
 class RefError(Exception):
     pass
+
+
+def ref_csr_convert(interchange_path, native_path, variant="generic"):
+    """The reference's csr_layout::convert; returns (status, message)."""
+    L = ref_lib(variant)
+    rc = L.ref_csr_convert(str(interchange_path).encode(), str(native_path).encode())
+    return rc, (L.ref_last_error().decode() if rc else "")
 
 
 class RefIndex:
@@ -229,6 +238,10 @@ class RefIndex:
 
     def write(self, path):
         self._check(self.L.ref_write_index(self.h, str(path).encode()))
+
+    def read_csr(self, path, residency=0):
+        """Index::read_csr; residency 1 = Residency::kMmap."""
+        self._check(self.L.ref_read_csr(self.h, str(path).encode(), int(residency)))
 
     @classmethod
     def read(cls, path, flags=0, variant="generic"):

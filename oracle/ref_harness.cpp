@@ -35,6 +35,7 @@
 #include "nsparse/seismic_index.h"
 #include "nsparse/seismic_scalar_quantized_index.h"
 #include "nsparse/sparse_vectors.h"
+#include "nsparse/utils/csr_layout.h"
 #include "nsparse/utils/scalar_quantizer.h"
 #include "nsparse/utils/vector_process.h"
 
@@ -163,6 +164,19 @@ int ref_write_index(void* h, const char* path) {
         nsparse::write_index(static_cast<nsparse::Index*>(h),
                              const_cast<char*>(path));
     });
+}
+
+// Index::read_csr with a residency: 0 in-memory, 1 mmap.
+int ref_read_csr(void* h, const char* path, int residency) {
+    return guarded([&] {
+        static_cast<nsparse::Index*>(h)->read_csr(
+            path, residency == 1 ? nsparse::Residency::kMmap : nsparse::Residency::kInMemory);
+    });
+}
+
+// csr_layout::convert: interchange CSR file -> native (.mcsr) file.
+int ref_csr_convert(const char* interchange_path, const char* native_path) {
+    return guarded([&] { nsparse::csr_layout::convert(interchange_path, native_path); });
 }
 
 void* ref_read_index(const char* path, int io_flags) {
