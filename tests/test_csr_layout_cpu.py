@@ -214,3 +214,29 @@ def test_quantized_index_refuses_the_mapped_residency(tmp_path):
     spec = "seismic_sq,quantizer=8bit|vmin=0.0|vmax=2.0|lambda=10|beta=2|alpha=0.4|seed=1"
     assert _ours_read(4, tmp_path / "m.mcsr", 1, spec) is ValueError
     assert _ref_read(4, tmp_path / "m.mcsr", 1, spec) is ValueError
+
+
+@need_ref
+@pytest.mark.parametrize("spec", [
+    "brutal", "inverted", "idmap,seismic,lambda=10|beta=2|alpha=0.4|seed=1",
+    "seismic_sq,quantizer=8bit|vmin=0.0|vmax=2.0|lambda=10|beta=2|alpha=0.4|seed=1",
+    "seismic,lambda=10|beta=2|alpha=0.4|seed=1"])
+def test_read_csr_layout_and_residency_matrix(tmp_path, spec):
+    """Every index type, either layout, either residency: loads the same
+    vectors or raises the same exception class as the reference (only a
+    seismic index reads the native layout, and only under kMmap)."""
+    write_interchange(tmp_path / "i.csr", 2, 4, 2, [0, 1, 2], [0, 3], [1.0, 2.0])
+    write_native(tmp_path / "n.mcsr", 2, 4, 2, [0, 1, 2], [0, 3], [1.0, 2.0])
+    for path in (tmp_path / "i.csr", tmp_path / "n.mcsr"):
+        for res in (0, 1):
+            idx = nsparse.index_factory(4, spec)
+            try:
+                idx.read_csr(path, res)
+                ours = idx.num_vectors()
+            except Exception as e:  # noqa: BLE001
+                ours = type(e)
+            r = O.RefIndex(4, spec)
+            rc = r.L.ref_read_csr(r.h, str(path).encode(), res)
+            ref = r.num_vectors() if rc == 0 else ERRORS[rc]
+            r.close()
+            assert ours == ref, (path.name, res)
