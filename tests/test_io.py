@@ -97,3 +97,24 @@ def test_unknown_fourcc_is_rejected(tmp_path):
 def test_missing_file(tmp_path):
     with pytest.raises(RuntimeError, match="Failed to open"):
         nsparse.read_index(str(tmp_path / "nope.idx"))
+
+
+@need_ref
+@pytest.mark.parametrize("bits", [8, 16])
+def test_quantized_add_writes_the_reference_codes(tmp_path, bits):
+    """A quantized index encodes on add, on the host: with either code width
+    the unbuilt index this engine writes is the reference's byte for byte
+    (header with quantizer type and range, codes, CSR layout), including
+    values outside the range (clamped) and at its ends."""
+    docs, _ = golden_corpus()
+    vals = docs.values.copy()
+    vals[:4] = [-1.0, 0.0, 1e9, float(docs.values.max())]
+    docs = type(docs)(docs.dim, docs.indptr, docs.indices, vals)
+    vmin, vmax = 0.05, 9.5
+    spec = (f"seismic_sq,quantizer={bits}bit|vmin={vmin!r}|vmax={vmax!r}|"
+            "lambda=200|beta=20|alpha=0.4|seed=7")
+    ref_index(docs, spec, build=False).write(str(tmp_path / "r.idx"))
+    ours = nsparse.index_factory(docs.dim, spec)
+    ours.add(docs.n, docs.indptr, docs.indices, docs.values)
+    nsparse.write_index(ours, str(tmp_path / "o.idx"))
+    assert open(tmp_path / "o.idx", "rb").read() == open(tmp_path / "r.idx", "rb").read()
