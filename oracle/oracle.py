@@ -165,6 +165,7 @@ def ref_lib(variant: str = "generic"):
         L.ref_write_index.argtypes = [P, ctypes.c_char_p]
         L.ref_read_csr.argtypes = [P, ctypes.c_char_p, ctypes.c_int]
         L.ref_csr_convert.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+        L.ref_factory_status.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p]
         L.ref_read_index.restype = P
         L.ref_read_index.argtypes = [ctypes.c_char_p, ctypes.c_int]
         L.ref_set_threads.argtypes = [ctypes.c_int]

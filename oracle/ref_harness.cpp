@@ -91,6 +91,16 @@ void* ref_index_factory(int dim, const char* desc) {
     return out;
 }
 
+// index_factory's outcome as a status (0 ok, else the guarded() code) and,
+// on success, the index's fourcc in out4.
+int ref_factory_status(int dim, const char* desc, char* out4) {
+    return guarded([&] {
+        std::unique_ptr<nsparse::Index> idx(nsparse::index_factory(dim, desc));
+        const auto id = idx->id();
+        std::memcpy(out4, id.data(), 4);
+    });
+}
+
 void ref_index_free(void* h) { delete static_cast<nsparse::Index*>(h); }
 
 int ref_add(void* h, int32_t n, const int32_t* indptr, const uint16_t* indices,
