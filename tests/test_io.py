@@ -118,3 +118,20 @@ def test_quantized_add_writes_the_reference_codes(tmp_path, bits):
     ours.add(docs.n, docs.indptr, docs.indices, docs.values)
     nsparse.write_index(ours, str(tmp_path / "o.idx"))
     assert open(tmp_path / "o.idx", "rb").read() == open(tmp_path / "r.idx", "rb").read()
+
+
+@need_ref
+@pytest.mark.parametrize("delegate", [
+    "seismic,lambda=200|beta=20|alpha=0.4|seed=7", "inverted",
+    "seismic_sq,quantizer=16bit|vmin=0.1|vmax=8|lambda=200|beta=20|alpha=0.4|seed=7"])
+def test_idmap_add_with_ids_writes_the_reference_file(tmp_path, delegate):
+    """add_with_ids on an IDMapIndex, written before any build: the external
+    id table and the delegate's vectors equal the reference's byte for byte."""
+    docs, _ = golden_corpus()
+    ids = np.arange(docs.n, dtype=np.int32) * 13 + 5
+    spec = "idmap," + delegate
+    ours = nsparse.index_factory(docs.dim, spec)
+    ours.add_with_ids(docs.n, docs.indptr, docs.indices, docs.values, ids)
+    nsparse.write_index(ours, str(tmp_path / "o.idx"))
+    ref_index(docs, spec, build=False, ids=ids).write(str(tmp_path / "r.idx"))
+    assert open(tmp_path / "o.idx", "rb").read() == open(tmp_path / "r.idx", "rb").read()
