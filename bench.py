@@ -219,7 +219,7 @@ def run_reference(args):
     r.build()
     build_s = time.perf_counter() - t
     log(f"reference build {build_s:.1f}s on {cores} threads")
-    sample = 2000  # queries per step: ~10-30 s of CPU work
+    sample = min(2000, qs.n)  # queries per step: ~10-30 s of CPU work at the full workload
     q = qs.rows(0, sample)
     for _ in range(args.warmup):
         r.search(q.rows(0, 200), K, param_kind=2, cut=CUT, heap_factor=HF)
@@ -229,7 +229,7 @@ def run_reference(args):
         r.search(q, K, param_kind=2, cut=CUT, heap_factor=HF)
         times.append(time.perf_counter() - t)
     value = sample * len(times) / sum(times)
-    lat = ref_per_query_latency(O.ref_lib(variant), r, q, 200, cores)
+    lat = ref_per_query_latency(O.ref_lib(variant), r, q, min(200, sample), cores)
     out = {"metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": 0, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": 1000 * sum(times) / len(times),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
