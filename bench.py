@@ -222,7 +222,7 @@ def run_reference(args):
     sample = min(2000, qs.n)  # queries per step: ~10-30 s of CPU work at the full workload
     q = qs.rows(0, sample)
     for _ in range(args.warmup):
-        r.search(q.rows(0, 200), K, param_kind=2, cut=CUT, heap_factor=HF)
+        r.search(q.rows(0, min(200, sample)), K, param_kind=2, cut=CUT, heap_factor=HF)
     times = []
     for _ in range(args.steps):
         t = time.perf_counter()
@@ -364,7 +364,7 @@ def run_engine(args):
     # ---- plain per-query path on a sample, and recall vs exact
     plain = nsparse.SeismicSearchParameters(CUT, HF)
     plain.set_engine(plain=True)
-    n_plain = 300
+    n_plain = min(300, qs.n)
     qp = qs.rows(0, n_plain)
     idx.search(qp.rows(0, 4).n, qp.rows(0, 4).indptr, qp.rows(0, 4).indices, qp.rows(0, 4).values,
                K, plain)
@@ -402,7 +402,7 @@ def run_engine(args):
             with tempfile.TemporaryDirectory() as td:
                 fpath = os.path.join(td, "c1.idx")
                 nsparse.write_index(idx, fpath)
-                cpu = cpu_baseline(docs, qs, fpath, 2000)
+                cpu = cpu_baseline(docs, qs, fpath, min(2000, qs.n))
         lat_ms = sorted(1000 * x for x in lat)
         out = {
             "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
