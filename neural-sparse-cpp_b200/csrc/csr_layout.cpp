@@ -34,12 +34,12 @@ void write_bytes(std::ofstream& f, const void* src, size_t n, const std::string&
     if (!f) throw std::runtime_error("Failed writing CSR file: " + path);
 }
 
-}  // namespace
-
 void read_bytes(std::ifstream& f, void* dst, size_t n, const std::string& path) {
     f.read(static_cast<char*>(dst), static_cast<std::streamsize>(n));
     if (!f) throw std::runtime_error("Truncated CSR file: " + path);
 }
+
+}  // namespace
 
 std::string native_path(const std::string& path) { return path + kNativeSuffix; }
 
