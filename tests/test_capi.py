@@ -208,3 +208,18 @@ def test_read_csr_errors(tmp_path):
         np.array([0.5, 0.25, 1.0], np.float32).tofile(f)
     with pytest.raises(ValueError, match="out of range"):
         nsparse.index_factory(64, "brutal").read_csr(str(bad))
+
+
+def test_import_fails_loudly_without_the_engine_library(tmp_path):
+    """No fallback: a copy of the Python package with no built library beside
+    it refuses to import."""
+    import shutil
+    import subprocess
+    import sys
+    src = os.path.join(ROOT, "neural-sparse-cpp_b200", "python", "nsparse")
+    dst = tmp_path / "pkg" / "python" / "nsparse"
+    shutil.copytree(src, dst, ignore=shutil.ignore_patterns("__pycache__"))
+    r = subprocess.run([sys.executable, "-c", "import nsparse"], cwd=str(dst.parent),
+                       capture_output=True, text=True)
+    assert r.returncode != 0
+    assert "ImportError" in r.stderr and "engine library not found" in r.stderr
