@@ -174,19 +174,29 @@ nsp_status_t nsp_index_search_device(nsp_index_t* index, int32_t n, const int32_
  * For callers that cannot allocate device memory per call: an engine
  * embedded in a host whose allocator accounts for every device byte against
  * a fixed budget, or a latency-critical loop that cannot afford
- * cudaMalloc/cudaFree, which can synchronize the device. Same arguments and
- * results as nsp_index_search_device, plus `nnz` (= d_indptr[n], the number
- * of query entries). The kernel's scratch (work counter, encoded query codes,
- * per-warp block-score rows) lives in a fixed device array of
+ * cudaMalloc/cudaFree, which can synchronize the device. Same arguments,
+ * kernel and results as nsp_index_search_device (the default one-CTA-per-query
+ * kernel, the index's autotuned launch shape, the knobs of `params`), plus:
+ *   - `nnz`: the number of query entries, d_indptr[n]. The call reads and
+ *     (quantized index) encodes exactly nnz values; a row that ends past nnz
+ *     is treated like a row longer than max_row_nnz (below).
+ *   - `d_status` (device int32, may be NULL): set to 0 by the call and to 3
+ *     by the kernel when a row is longer than max_row_nnz or ends past nnz;
+ *     such rows return padding. Read it after synchronizing the stream.
+ * The search's scratch (work counter, counters, encoded query codes,
+ * block-score rows, visiting orders) lives in a fixed device array of
  * NSP_NOALLOC_SCRATCH_BYTES that every GPU loading the library reserves until
- * exit; no cudaMalloc, cudaFree or allocating library routine is called.
+ * exit; no cudaMalloc, cudaFree or allocating library routine is called. The
+ * grid is capped to the CTAs whose scratch fits the array.
+ *   - `cuda_stream` NULL is the legacy default stream.
  *   - The first call on a device looks up that array's device address (set-up
  *     once per device); make that first call before any stream capture.
  *   - The index must already be resident on the GPU (one ordinary search or a
  *     build followed by a search does that); otherwise the call is rejected.
  *   - Rejected with NSP_ERR_INVALID_ARGUMENT: an id selector, plain mode, or a
- *     batch whose codes (2*nnz bytes) or block-score rows (4 bytes per block of
- *     the largest posting list, per warp) do not fit the array.
+ *     batch whose codes (2*nnz bytes) or the block-score rows of one CTA (4
+ *     bytes per block of the largest posting list, per warp) do not fit the
+ *     array.
  *   - All calls share the array and it keeps the last call's contents: calls
  *     that overlap on the GPU (other streams, other host threads) race; order
  *     them on one stream. */
@@ -196,7 +206,7 @@ nsp_status_t nsp_index_search_device_noalloc(nsp_index_t* index, int32_t n,
                                              const float* d_values, int32_t nnz,
                                              int32_t max_row_nnz, int k, float* d_distances,
                                              int32_t* d_labels, const nsp_search_params_t* params,
-                                             void* cuda_stream);
+                                             void* cuda_stream, int32_t* d_status);
 
 /* Kernel autotuner. Times each one-CTA-per-query launch shape of the SEISMIC
  * search (lanes per doc, candidate docs per batch, warps per CTA) on the n

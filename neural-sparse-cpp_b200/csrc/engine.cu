@@ -585,6 +585,8 @@ SeismicPlan plan_seismic_cta(int kind, int dim, int qcap, int k, int n_queries,
     // whole clusters; a persistent grid of at most one resident wave
     const int slots = std::max(1, device_sm_count() * per_sm / cl);
     p.blocks = single ? cl : std::max(1, std::min(n_queries, slots)) * cl;
+    if (args.max_ctas > 0 && !single)
+        p.blocks = std::max(cl, std::min(p.blocks, args.max_ctas / cl * cl));
     return p;
 }
 
@@ -616,6 +618,7 @@ SeismicPlan plan_seismic(int kind, int words, int qcap, int k, int n_queries,
     if (per_sm < 1) per_sm = 1;
     const int want = (n_queries + wpb - 1) / wpb;
     p.blocks = std::max(1, std::min(want, device_sm_count() * per_sm));
+    if (args.max_ctas > 0) p.blocks = std::min(p.blocks, args.max_ctas);
     return p;
 }
 
@@ -654,6 +657,7 @@ void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
     a.out_d = d_out;
     a.out_l = d_lab;
     a.qcap = std::max(qcap, 1);
+    a.nnz_cap = args.nnz_cap;
     auto* st = static_cast<unsigned long long*>(
         ws.dev(Workspace::kStats, kStatCount * sizeof(unsigned long long)));
     cuda_check(cudaMemsetAsync(st, 0, kStatCount * sizeof(unsigned long long), s), "memset");
@@ -770,6 +774,37 @@ void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
     }
+}
+
+SeismicScratchNeed seismic_scratch_need(const ForwardDevice& fwd, const SeismicDevice& ix,
+                                        int32_t n, int32_t max_nnz,
+                                        const SeismicSearchArgs& args_in) {
+    SeismicSearchArgs args = args_in;
+    if (args.variant < 0) args.variant = kDefaultVariant;
+    if (args.plain) throw std::invalid_argument("scratch of a batched search only");
+    const int kind = val_kind_of(args.qbits);
+    const int qcap = std::max(max_nnz, 1);
+    const int maxb = std::max(ix.max_blocks(), 1);
+    SeismicScratchNeed need;
+    // stats, error word, work counter (run_seismic asks for each)
+    need.fixed = kStatCount * sizeof(unsigned long long) + 2 * sizeof(int32_t);
+    if (args.variant >= 2) {
+        const SeismicPlan p = plan_seismic_cta(kind, fwd.view().dim, qcap, args.k, n, args, false);
+        int p2 = 1;
+        while (p2 < maxb) p2 <<= 1;
+        need.per_cta = static_cast<size_t>(p.wpb) * maxb * sizeof(float) +
+                       static_cast<size_t>((maxb + 7) & ~7) * sizeof(uint16_t) +
+                       (p2 > 2 * p.batch_docs ? static_cast<size_t>(p2) * 8 : 0);
+        need.ctas = p.blocks;
+        need.cluster = p.cluster;
+    } else {
+        const int words = (fwd.view().dim + 31) / 32;
+        const SeismicPlan p = plan_seismic(kind, words, qcap, args.k, n, args, ix.max_blocks());
+        need.per_cta = static_cast<size_t>(p.wpb) * ix.max_blocks() * sizeof(float);
+        need.ctas = p.blocks;
+        need.cluster = 1;
+    }
+    return need;
 }
 
 void reserve_seismic_scratch(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,

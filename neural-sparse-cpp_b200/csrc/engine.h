@@ -287,7 +287,21 @@ struct SeismicSearchArgs {
     // variants 2-5: one device doc bitmap per query (a null entry admits every
     // doc), in device memory; replaces the launch-wide selector
     const uint64_t* const* d_sel_q = nullptr;
+    int max_ctas = 0;         // cap on the persistent grid's CTAs (0: none)
+    int32_t nnz_cap = -1;     // entries the query arrays hold (negative: not checked)
 };
+
+// Device scratch a batched (not plain) run_seismic of `n` queries with `args`
+// asks for: `fixed` bytes whatever the grid, plus `per_cta` for each of the
+// `ctas` CTAs of its grid (a whole number of `cluster`-CTA clusters).
+struct SeismicScratchNeed {
+    size_t fixed = 0;
+    size_t per_cta = 0;
+    int ctas = 0;
+    int cluster = 1;
+};
+SeismicScratchNeed seismic_scratch_need(const ForwardDevice& fwd, const SeismicDevice& ix,
+                                        int32_t n, int32_t max_nnz, const SeismicSearchArgs& args);
 
 // Host buffers in, host buffers out (the reference-facing path).
 void seismic_search(const ForwardDevice& fwd, const SeismicDevice& ix, const QueryBatch& q,

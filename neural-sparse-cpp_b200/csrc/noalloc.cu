@@ -4,12 +4,18 @@
 // serving process with admission control), or a latency-critical loop that
 // cannot afford cudaMalloc/cudaFree, which can synchronize the whole device.
 //
-// The search kernel's scratch (its work counter, the encoded query codes of a
-// quantized index, and the per-warp block-score rows) lives in the file-scope
-// device array below instead of the engine's per-thread workspace. Every GPU
-// that loads the library reserves kNoAllocScratchBytes for it until exit.
+// The search is the engine's ordinary batched search (run_seismic: the
+// one-CTA-per-query kernel unless the parameters ask for another, the
+// index's autotuned launch shape when they leave the choice to the engine),
+// with every scratch buffer it asks for -- work counter, counters, block-score
+// rows, visiting orders, sort keys, the encoded query codes of a quantized
+// index -- carved from the file-scope device array below instead of the
+// per-thread workspace. The grid is capped to the CTAs whose block-score rows
+// fit the array. Every GPU that loads the library reserves
+// kNoAllocScratchBytes for it until exit.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -51,6 +57,41 @@ void* scratch_on_current_device() {
 
 constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Hands out 256-byte aligned regions of one fixed device range in the order a
+// search asks for its scratch slots; a slot asked for again gets its region
+// back. The error slot is the caller's status word when one is given. Nothing
+// is allocated: a request beyond the range is refused.
+class FixedScratch final : public nsp::Scratch {
+public:
+    FixedScratch(unsigned char* base, size_t cap, int32_t* status)
+        : base_(base), cap_(cap), status_(status) {}
+    void* dev(int slot, size_t bytes) override {
+        if (slot == nsp::Workspace::kErr && status_ != nullptr) return status_;
+        if (slot < 0 || slot >= nsp::Workspace::kNumSlots)
+            throw std::runtime_error("unknown scratch slot");
+        if (ptr_[slot] != nullptr) {
+            if (bytes <= size_[slot]) return ptr_[slot];
+            throw std::runtime_error("scratch slot asked for more than its first request");
+        }
+        const size_t at = align256(used_);
+        if (at > cap_ || bytes > cap_ - at)
+            throw std::invalid_argument("query batch too large for the no-allocation scratch (" +
+                                        std::to_string(cap_) + " bytes)");
+        ptr_[slot] = base_ + at;
+        size_[slot] = bytes;
+        used_ = at + bytes;
+        return ptr_[slot];
+    }
+
+private:
+    unsigned char* base_;
+    size_t cap_;
+    int32_t* status_;
+    size_t used_ = 0;
+    void* ptr_[nsp::Workspace::kNumSlots] = {};
+    size_t size_[nsp::Workspace::kNumSlots] = {};
+};
+
 }  // namespace
 
 namespace nsp {
@@ -60,7 +101,7 @@ void set_last_error(const char* msg);  // capi.cpp
 extern "C" nsp_status_t nsp_index_search_device_noalloc(
     nsp_index_t* index, int32_t n, const int32_t* d_indptr, const uint16_t* d_indices,
     const float* d_values, int32_t nnz, int32_t max_row_nnz, int k, float* d_distances,
-    int32_t* d_labels, const nsp_search_params_t* params, void* cuda_stream) {
+    int32_t* d_labels, const nsp_search_params_t* params, void* cuda_stream, int32_t* d_status) {
     using namespace nsparse;
     try {
         if (index == nullptr || d_indptr == nullptr || d_indices == nullptr ||
@@ -80,9 +121,17 @@ extern "C" nsp_status_t nsp_index_search_device_noalloc(
         if (ssp->cut <= 0) throw std::invalid_argument("value must be positive");
 
         detail::SeismicState* st = nullptr;
-        int val_kind = nsp::kF32;
-        int qbits = 0;
-        float q_vmin = 0.0F, q_scale = 0.0F, decode = 0.0F;
+        nsp::SeismicSearchArgs a;
+        a.k = k;
+        a.cut = ssp->cut;
+        a.heap_factor = ssp->heap_factor;
+        if (sp != nullptr) {
+            a.variant = sp->engine.variant;
+            a.warps_per_block = sp->engine.warps_per_block;
+            a.stage_bytes = sp->engine.stage_bytes;
+            a.batch_docs = sp->engine.batch_docs;
+            a.cluster = sp->engine.ctas_per_query;
+        }
         if (auto* si = dynamic_cast<SeismicIndex*>(base)) {
             st = si->state();
         } else if (auto* qi = dynamic_cast<SeismicScalarQuantizedIndex*>(base)) {
@@ -91,11 +140,10 @@ extern "C" nsp_status_t nsp_index_search_device_noalloc(
             const auto* sqp = dynamic_cast<const SeismicSQSearchParameters*>(sp);
             const ScalarQuantizer qsq =
                 sqp == nullptr ? isq : ScalarQuantizer(isq.get_quantizer_type(), sqp->vmin, sqp->vmax);
-            qbits = isq.bits();
-            val_kind = qbits == 8 ? nsp::kU8 : nsp::kU16;
-            q_vmin = qsq.get_min();
-            q_scale = qsq.encode_scale();
-            decode = isq.decode_scale(qsq);
+            a.qbits = isq.bits();
+            a.q_vmin = qsq.get_min();
+            a.q_scale = qsq.encode_scale();
+            a.decode_scale = isq.decode_scale(qsq);
         } else {
             throw std::invalid_argument("the no-allocation search supports seismic indexes");
         }
@@ -104,59 +152,55 @@ extern "C" nsp_status_t nsp_index_search_device_noalloc(
         if (st->vectors.dirty || st->vectors.dev.empty() || !st->dev_valid)
             throw std::invalid_argument(
                 "index is not resident on the GPU: run one ordinary search first");
+        detail::apply_tuned(*st, a, n);
+        // every row must end within the nnz entries the caller declared
+        a.nnz_cap = nnz;
 
-        nsp::SeismicLaunch a{};
-        a.fwd = st->vectors.dev.view();
-        a.ix = st->lists_dev.view();
-        a.ix.words = (a.fwd.dim + 31) / 32;
-        a.q.n = n;
-        a.q.indptr = d_indptr;
-        a.q.idx = d_indices;
-        a.k = k;
-        a.cut = ssp->cut;
-        a.heap_factor = ssp->heap_factor;
-        a.decode_scale = decode;
-        a.out_d = d_distances;
-        a.out_l = d_labels;
-        a.qcap = max_row_nnz > 0 ? max_row_nnz : 1;
-        a.stats = nullptr;
-        a.first_query = 0;
-
-        // scratch layout: [counter | query codes | block-score rows]
         auto* scratch = static_cast<unsigned char*>(scratch_on_current_device());
-        const size_t codes_bytes = qbits == 0 ? 0 : align256(static_cast<size_t>(nnz) * 2 + 16);
-        const size_t head = 256 + codes_bytes;
-        if (head >= kNoAllocScratchBytes)
+        size_t head = 0;
+        const void* vals = d_values;
+        auto* stream = static_cast<cudaStream_t>(cuda_stream);
+        // the encoded query codes of a quantized index come first
+        const size_t codes_bytes =
+            a.qbits == 0 ? 0 : align256(static_cast<size_t>(nnz) * 2 + 16);
+        if (codes_bytes + 4096 > kNoAllocScratchBytes)
             throw std::invalid_argument("query batch too large for the no-allocation scratch (" +
                                         std::to_string(kNoAllocScratchBytes) + " bytes)");
-        const size_t row_bytes = static_cast<size_t>(a.ix.max_blocks) * sizeof(float);
-        const size_t rows = (kNoAllocScratchBytes - head) / row_bytes;
-        if (rows < 1)
-            throw std::invalid_argument("posting lists have too many blocks for the no-allocation "
-                                        "scratch");
-        const size_t per_warp = nsp::seismic_smem_per_warp(val_kind, a.ix.words, a.qcap, k);
-        int wpb = 4;
-        while (wpb > 1 && static_cast<size_t>(wpb) > rows) wpb >>= 1;
-        int per_sm = nsp::seismic_max_blocks_per_sm(val_kind, wpb, per_warp * wpb);
-        if (per_sm < 1) per_sm = 1;
-        long long blocks_ll = std::min<long long>((n + wpb - 1) / wpb,
-                                                  static_cast<long long>(nsp::device_sm_count()) * per_sm);
-        blocks_ll = std::min<long long>(blocks_ll, static_cast<long long>(rows / wpb));
-        int blocks = static_cast<int>(blocks_ll);
-        if (blocks < 1) blocks = 1;
-
-        auto* stream = static_cast<cudaStream_t>(cuda_stream);
-        a.work_counter = reinterpret_cast<int32_t*>(scratch);
-        nsp::cuda_check(cudaMemsetAsync(a.work_counter, 0, sizeof(int32_t), stream), "memset");
-        a.q.val = d_values;
-        if (qbits != 0) {
-            void* codes = scratch + 256;
-            nsp::cuda_check(nsp::launch_sq_encode(d_values, codes, nnz, qbits, q_vmin, q_scale, stream),
-                            "query encode");
-            a.q.val = codes;
+        head = codes_bytes;
+        const size_t avail = kNoAllocScratchBytes - head;
+        // The grid: as many CTAs as the engine would launch, capped to what
+        // the rest of the array holds (one slack region of 256 bytes per
+        // scratch slot for alignment).
+        nsp::SeismicScratchNeed need = nsp::seismic_scratch_need(
+            st->vectors.dev, st->lists_dev, n, max_row_nnz, a);
+        const size_t slack = 8 * 256;
+        auto fits = [&](const nsp::SeismicScratchNeed& nd) -> long long {
+            if (nd.fixed + slack >= avail || nd.per_cta == 0) return 0;
+            return static_cast<long long>((avail - nd.fixed - slack) / nd.per_cta);
+        };
+        long long room = fits(need);
+        if (room < need.cluster && need.cluster > 1 && a.cluster <= 0) {
+            // the engine's cluster does not fit: one CTA per query
+            a.cluster = 1;
+            need = nsp::seismic_scratch_need(st->vectors.dev, st->lists_dev, n, max_row_nnz, a);
+            room = fits(need);
         }
-        a.bscore = reinterpret_cast<float*>(scratch + head);
-        nsp::cuda_check(nsp::launch_seismic(val_kind, a, wpb, blocks, stream), "seismic search");
+        if (room < need.cluster)
+            throw std::invalid_argument("posting lists have too many blocks for the no-allocation "
+                                        "scratch (" + std::to_string(kNoAllocScratchBytes) +
+                                        " bytes)");
+        a.max_ctas = static_cast<int>(std::min<long long>(room, need.ctas));
+
+        FixedScratch fixed(scratch + head, avail, d_status);
+        if (a.qbits != 0) {
+            void* codes = scratch;
+            nsp::cuda_check(
+                nsp::launch_sq_encode(d_values, codes, nnz, a.qbits, a.q_vmin, a.q_scale, stream),
+                "query encode");
+            vals = codes;
+        }
+        nsp::run_seismic(st->vectors.dev, st->lists_dev, n, d_indptr, d_indices, vals,
+                         max_row_nnz, a, nullptr, d_distances, d_labels, stream, fixed, nullptr);
         return NSP_OK;
     } catch (const std::invalid_argument& e) {
         nsp::set_last_error(e.what());

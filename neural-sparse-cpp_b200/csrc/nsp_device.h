@@ -116,6 +116,10 @@ struct SeismicLaunch {
     // walking the query and every CTA scoring its batches.
     int32_t seg_cap;
     int32_t cluster;
+    // Entries the query arrays hold (negative: not checked). A row that ends
+    // past it is treated as empty and reported through `err`, like a row
+    // longer than qcap.
+    int32_t nnz_cap;
 };
 
 // Doc-ascending postings of an fp32 forward index (the exact search's

@@ -599,7 +599,14 @@ __device__ bool run_query(const SeismicLaunch& a, const WarpSlice<V>& w, float* 
     bool ok = true;
     const int words = a.ix.words;
     const int32_t qs = a.q.indptr[q];
-    const int qn = a.q.indptr[q + 1] - qs;
+    int qn = a.q.indptr[q + 1] - qs;
+    // The warp's shared slice holds a.qcap query entries. A longer row (the
+    // caller's max_nnz was wrong) or one past the query arrays is treated as
+    // empty -- padding -- and reported.
+    if (qn > a.qcap || qn < 0 || qs < 0 || (a.nnz_cap >= 0 && qs + qn > a.nnz_cap)) {
+        if (lane == 0 && a.err != nullptr) atomicExch(a.err, 3);
+        qn = 0;
+    }
     const uint16_t* gq_idx = a.q.idx + qs;
     const V* gq_val = static_cast<const V*>(a.q.val) + qs;
 

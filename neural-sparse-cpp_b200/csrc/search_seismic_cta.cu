@@ -648,7 +648,9 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                 if (q >= a.q.n) break;
                 const int32_t qs = a.q.indptr[q];
                 int qn = a.q.indptr[q + 1] - qs;
-                if (qn > a.qcap || qn < 0) qn = 0;  // the leader reports it
+                // the leader reports it
+                if (qn > a.qcap || qn < 0 || qs < 0 || (a.nnz_cap >= 0 && qs + qn > a.nnz_cap))
+                    qn = 0;
                 bool bad = false;
                 for (int i = tid; i < qn; i += blockDim.x) {
                     const uint32_t t = a.q.idx[qs + i];
@@ -710,8 +712,10 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
         // 1. scatter the query
         const int32_t qs = a.q.indptr[q];
         int qn = a.q.indptr[q + 1] - qs;
-        if (qn > a.qcap || qn < 0) {  // the caller's max_nnz was wrong: padding
-            if (tid == 0) atomicExch(a.err, 3);
+        // the caller's max_nnz was wrong, or the row lies past the query
+        // arrays: padding, and the error is reported
+        if (qn > a.qcap || qn < 0 || qs < 0 || (a.nnz_cap >= 0 && qs + qn > a.nnz_cap)) {
+            if (tid == 0 && a.err != nullptr) atomicExch(a.err, 3);
             qn = 0;
         }
         bool bad = false;
