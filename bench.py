@@ -150,9 +150,11 @@ def replica_throughput(total_ms, e2e_s, n_queries, steps, e2e_steps, world, devi
     return total_ms, value, e2e_value
 
 
-def cpu_baseline(docs, qs, index_file, sample):
+def cpu_baseline(docs, qs, index_file, sample, D_eng=None, L_eng=None, gt_L=None):
     """The reference's own search (compiled from its sources, oracle/_ref), all
-    host threads, on the first `sample` queries of the workload."""
+    host threads, on the first `sample` queries of the workload; with the
+    engine's rows for the same queries, their parity with the reference's and
+    the reference's recall@10 at the same knobs."""
     import oracle as O
     variant = ref_variant()
     if variant is None:
@@ -164,14 +166,19 @@ def cpu_baseline(docs, qs, index_file, sample):
     q = qs.rows(0, sample)
     r.search(q.rows(0, min(64, sample)), K, param_kind=2, cut=CUT, heap_factor=HF)  # warm
     t = time.perf_counter()
-    r.search(q, K, param_kind=2, cut=CUT, heap_factor=HF)
+    Dr, Lr = r.search(q, K, param_kind=2, cut=CUT, heap_factor=HF)
     dt = time.perf_counter() - t
     lat = ref_per_query_latency(L, r, q, min(200, sample), cores)
     r.close()
-    return {"value": sample / dt, "unit": "queries/s", "cores": cores, "kind": "reference",
-            "sample": f"{sample} of the {N_QUERIES} queries, one batched search() call, "
-                      f"reference {variant} build, OMP threads={cores}",
-            "per_query_1_thread": lat}
+    out = {"value": sample / dt, "unit": "queries/s", "cores": cores, "kind": "reference",
+           "sample": f"{sample} of the {N_QUERIES} queries, one batched search() call, "
+                     f"reference {variant} build, OMP threads={cores}",
+           "per_query_1_thread": lat}
+    if L_eng is not None:
+        out["parity"] = row_parity(D_eng[:sample], L_eng[:sample], Dr, Lr)
+    if gt_L is not None:
+        out["reference_recall_at_10"] = recall_at_k(Lr, gt_L[:sample])
+    return out
 
 
 def ref_per_query_latency(L, r, q, n, cores):
@@ -402,7 +409,7 @@ def run_engine(args):
             with tempfile.TemporaryDirectory() as td:
                 fpath = os.path.join(td, "c1.idx")
                 nsparse.write_index(idx, fpath)
-                cpu = cpu_baseline(docs, qs, fpath, min(2000, qs.n))
+                cpu = cpu_baseline(docs, qs, fpath, min(2000, qs.n), D, L, Lt)
         lat_ms = sorted(1000 * x for x in lat)
         out = {
             "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
@@ -437,76 +444,171 @@ def run_engine(args):
         torch.distributed.destroy_process_group()
 
 
-# SEISMIC-SQ at 8.8M docs: uint8 codes, uneven queries (nnz 5-200), posting
-# cap 6,000, 600 blocks per full list; (query cut, heap factor) swept: the
-# workload's cut 12 with heap factors 0.7-0.95, then wider cuts.
+# SEISMIC-SQ at 8.8M docs -- the hot path's target workload: uint8 codes
+# (per-index min/max scale), queries of 5-200 terms, posting cap 6,000, 600
+# blocks per full list, alpha 0.4, query cut 12, heap factor 0.9; 65,536
+# queries per step in launches of 16,384.
 SQ_DOCS = 8_800_000
 SQ_QUERIES = 65_536
 SQ_BATCH = 16_384
-SQ_SWEEP = ((12, 0.7), (12, 0.8), (12, 0.9), (12, 0.95), (20, 0.9), (30, 0.9), (40, 0.9))
-SQ_GT_QUERIES = 1000
+SQ_CUT, SQ_HF = 12, 0.9
+SQ_QUERY_SEED, SQ_TUNE_SEED = 2000, 2001  # timed queries; the autotuner's own sample
+SQ_GT_QUERIES = 1000   # recall against exact search, and the reference's parity rows
+SQ_CPU_SAMPLE = 2000   # queries per reference CPU search
 SQ_PLAIN = 200
+SQ_METRIC = "QPS@recall@10≥0.95 batched vs per-query on 1 B200; p50/p99 ms; HBM GB/s"
+
+
+def sq_spec_for(vmin, vmax):
+    return (f"seismic_sq,quantizer=8bit|vmin={vmin!r}|vmax={vmax!r}|lambda=6000|beta=600|"
+            f"alpha=0.4|seed=7")
+
+
+def sq_data(n_docs, rank):
+    from nsparse_b200 import synth
+    docs = synth.docs_config2(n_docs, seed=0)
+    qs = synth.queries_config2(SQ_QUERIES, seed=SQ_QUERY_SEED + 100 * rank)
+    return docs, qs
+
+
+def sq_workload(docs, qs, hf=SQ_HF, cut=SQ_CUT):
+    return {"workload": f"seismic_sq8_{docs.n}_docs_{qs.n}_queries", "docs": docs.n,
+            "nnz": int(docs.nnz), "vocab": docs.dim, "queries": qs.n, "batch": SQ_BATCH,
+            "query_nnz": "uniform 5-200", "quantizer": "8bit, per-index min/max",
+            "lambda": 6000, "beta": 600, "alpha": 0.4, "cut": cut, "heap_factor": hf, "k": K,
+            "l2": "flushed between steps; index > L2"}
+
+
+def row_parity(D, L, Dr, Lr):
+    """Engine rows against the reference's rows for the same queries and
+    index file. A row is tied when its engine scores repeat a value (the order
+    of equal scores is left unspecified by the reference); on the other rows
+    ids and scores must be identical."""
+    same = (L == Lr).all(axis=1) & (D == Dr).all(axis=1)
+    tied = np.array([len(set(d[l >= 0].tolist())) < int((l >= 0).sum()) for d, l in zip(D, L)])
+    same_scores = (np.sort(D, axis=1) == np.sort(Dr, axis=1)).all(axis=1)
+    untied = ~tied
+    mism = int(((L != Lr) | (D != Dr))[untied].any(axis=1).sum())
+    return {"rows": int(len(L)), "rows_identical_frac": float(same.mean()),
+            "rows_same_scores_frac": float(same_scores.mean()),
+            "untied_rows": int(untied.sum()),
+            "untied_rows_identical_frac": float(same[untied].mean()) if untied.any() else 1.0,
+            "score_mismatches_untied_rows": mism}
+
+
+def sq_reference_leg(index_file, qs, gt_L, D_eng, L_eng, vmin, vmax, cut, hf):
+    """The reference's own search (compiled from its sources, oracle/_ref) of
+    the index file the engine wrote: batched QPS on all host threads and
+    per-query single-thread latency (cpu_baseline), its recall@10 at the same
+    (cut, heap factor), and row parity with the engine."""
+    import oracle as O
+    variant = ref_variant()
+    if variant is None:
+        return None, None
+    L = O.ref_lib(variant)
+    cores = os.cpu_count()
+    L.ref_set_threads(cores)
+    t = time.perf_counter()
+    r = O.RefIndex.read(index_file, variant=variant)
+    read_s = time.perf_counter() - t
+    sample = min(SQ_CPU_SAMPLE, qs.n)
+    q = qs.rows(0, sample)
+    r.search(q.rows(0, 64), K, param_kind=2, cut=cut, heap_factor=hf)  # warm
+    t = time.perf_counter()
+    Dr, Lr = r.search(q, K, param_kind=2, cut=cut, heap_factor=hf)
+    dt = time.perf_counter() - t
+    n_gt = len(gt_L)
+    lat = _ref_latency(L, r, q, min(200, sample), cores, cut, hf)
+    r.close()
+    cpu = {"value": sample / dt, "unit": "queries/s", "cores": cores, "kind": "reference",
+           "sample": f"first {sample} of the {qs.n} queries, one batched search() call on the "
+                     f"engine-written index file, reference {variant} build, OMP threads={cores}",
+           "index_read_s": read_s, "per_query_1_thread": lat}
+    ref = {"recall_at_10": recall_at_k(Lr[:n_gt], gt_L),
+           "parity": row_parity(D_eng[:sample], L_eng[:sample], Dr, Lr)}
+    return cpu, ref
+
+
+def _ref_latency(L, r, q, n, cores, cut, hf):
+    """Per-query latency as the reference's residency benchmark takes it
+    (benchmarks/sq_residency_bench.cpp:249-269): one thread, one search()
+    call per query; p50/p99 over the first n queries."""
+    L.ref_set_threads(1)
+    try:
+        ms = []
+        for i in range(n):
+            one = q.rows(i, i + 1)
+            t = time.perf_counter()
+            r.search(one, K, param_kind=2, cut=cut, heap_factor=hf)
+            ms.append(1000.0 * (time.perf_counter() - t))
+    finally:
+        L.ref_set_threads(cores)
+    return {"queries": n, "p50_ms": float(np.percentile(ms, 50)),
+            "p99_ms": float(np.percentile(ms, 99)), "threads": 1}
 
 
 def run_engine_sq(args):
-    """SEISMIC-SQ workload: device build (seconds), then for each heap factor
-    the batched search of 65,536 queries in batches of 16,384 (device-resident
-    queries and results), recall@10 against exact fp32 ground truth on the
-    first 1,000 queries, and the one-query-per-launch path on 200 queries
-    (ids and scores identical to the batched path)."""
+    """The headline: SEISMIC-SQ at 8.8M docs on the device. Device build
+    (seconds); the batched search of 65,536 queries per step as four captured
+    16,384-query graph steps over device-resident queries and results
+    (`value`); the same through the host API with copies (`e2e`); the plain
+    one-query-per-call path through the same host API; recall@10 against exact
+    fp32 search and against the exact ranking of the codes; the reference's
+    CPU search of the engine-written file (cpu_baseline, its recall at the same
+    knobs, row parity); the serving loop's latency under Poisson arrivals."""
     import torch
-    torch.cuda.set_device(0)
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    else:
+        torch.cuda.set_device(0)
     import nsparse
     from nsparse_b200 import synth
-    dev = torch.device("cuda", 0)
+    dev = torch.device("cuda", torch.cuda.current_device())
     n_docs = args.docs or SQ_DOCS
     t = time.perf_counter()
-    docs = synth.docs_config2(n_docs, seed=0)
-    qs = synth.queries_config2(SQ_QUERIES, seed=2000)
-    log(f"generated {docs.n} docs ({docs.nnz} nnz) in {time.perf_counter() - t:.1f}s")
+    docs, qs = sq_data(n_docs, rank)
+    if args.queries:
+        qs = qs.rows(0, min(qs.n, args.queries))
+    log(f"rank {rank}: generated {docs.n} docs ({docs.nnz} nnz) in {time.perf_counter() - t:.1f}s")
     vmin, vmax = float(docs.values.min()), float(docs.values.max())
-    spec = (f"seismic_sq,quantizer=8bit|vmin={vmin!r}|vmax={vmax!r}|lambda=6000|beta=600|"
-            f"alpha=0.4|seed=7")
-    if args.kernel_only:
-        # build, then the batched search launches only (the profiling case)
-        idx = nsparse.index_factory(docs.dim, spec)
-        idx.add(docs.n, docs.indptr, docs.indices, docs.values)
-        idx.build()
-        params = nsparse.SeismicSearchParameters(12, 0.9)
-        params.set_kernel(args.variant, args.tuning)
-        q = qs.rows(0, SQ_BATCH)
-        for _ in range(max(args.warmup, 1) + args.steps):
-            idx.search(q.n, q.indptr, q.indices, q.values, K, params)
-        st = nsparse.last_search_stats()
-        print(json.dumps({"case": f"seismic_sq8_{docs.n}_docs_{q.n}_queries", "cut": 12,
-                          "heap_factor": 0.9, "kernel_ms": st.kernel_ms,
-                          "algorithmic_bytes": st.bytes,
-                          "docs_scored_per_query": st.docs_scored / q.n}))
-        return
-    # exact fp32 ground truth first (its index is freed before the SQ build)
-    t = time.perf_counter()
-    exact = nsparse.index_factory(docs.dim, "inverted")
-    exact.add(docs.n, docs.indptr, docs.indices, docs.values)
-    exact.build()
-    gt = qs.rows(0, SQ_GT_QUERIES)
-    _, Lt = exact.search(gt.n, gt.indptr, gt.indices, gt.values, K)
-    del exact
-    # exact ranking over the 8-bit codes themselves (integer scores, exact in
-    # fp32 below 2^24): separates SEISMIC's pruning from the quantizer's loss
-    scale = np.float32(255.0) / (np.float32(vmax) - np.float32(vmin))
+    spec = sq_spec_for(vmin, vmax)
+    cut, hf = SQ_CUT, SQ_HF
+    batch = min(SQ_BATCH, qs.n)
+    main = rank == 0 and not args.kernel_only
 
-    def codes(v):
-        x = (v.astype(np.float32) - np.float32(vmin)) * scale
-        return np.floor(np.clip(x, 0, 255) + np.float32(0.5)).astype(np.float32)
+    # ---- exact ground truth (rank 0): fp32 search, and the exact ranking of
+    # the codes (integer scores, exact in fp32 below 2^24) -- the latter
+    # separates SEISMIC's pruning from the quantizer's own loss
+    gt_L = Dc = None
+    n_gt = min(SQ_GT_QUERIES, qs.n)
+    gt = qs.rows(0, n_gt)
+    if main:
+        t = time.perf_counter()
+        exact = nsparse.index_factory(docs.dim, "inverted")
+        exact.add(docs.n, docs.indptr, docs.indices, docs.values)
+        exact.build()
+        _, gt_L = exact.search(gt.n, gt.indptr, gt.indices, gt.values, K)
+        del exact
+        scale = np.float32(255.0) / (np.float32(vmax) - np.float32(vmin))
 
+        def codes(v):
+            x = (v.astype(np.float32) - np.float32(vmin)) * scale
+            return np.floor(np.clip(x, 0, 255) + np.float32(0.5)).astype(np.float32)
+
+        exact = nsparse.index_factory(docs.dim, "inverted")
+        exact.add(docs.n, docs.indptr, docs.indices, codes(docs.values))
+        exact.build()
+        Dc, _ = exact.search(gt.n, gt.indptr, gt.indices, codes(gt.values), K)
+        del exact
+        log(f"exact ground truth {time.perf_counter() - t:.1f}s")
     rng_f = np.float32(vmax) - np.float32(vmin)
-    decode = float((rng_f * rng_f) / np.float32(255.0 * 255.0))  # SQ score per code unit
-    exact = nsparse.index_factory(docs.dim, "inverted")
-    exact.add(docs.n, docs.indptr, docs.indices, codes(docs.values))
-    exact.build()
-    Dc, _ = exact.search(gt.n, gt.indptr, gt.indices, codes(gt.values), K)
-    del exact
-    log(f"exact ground truth {time.perf_counter() - t:.1f}s")
+    decode = float((rng_f * rng_f) / np.float32(255.0 * 255.0))  # score per code unit
+
+    # ---- device build
     torch.cuda.synchronize()
     t = time.perf_counter()
     idx = nsparse.index_factory(docs.dim, spec)
@@ -514,115 +616,248 @@ def run_engine_sq(args):
     idx.build()
     torch.cuda.synchronize()
     build_s = time.perf_counter() - t
-    log(f"device build {build_s:.1f}s")
+    log(f"rank {rank}: device build {build_s:.1f}s")
+    params = nsparse.SeismicSearchParameters(cut, hf)
+    params.set_kernel(args.variant, args.tuning)
+    tuned = None
+    if args.variant < 0:
+        # the autotuner's sample is drawn apart from the timed queries
+        tq = synth.queries_config2(4096, seed=SQ_TUNE_SEED)
+        tuned = idx.autotune(tq.n, tq.indptr, tq.indices, tq.values, K, params)
+        log(f"autotune: {tuned}")
+
+    # ---- device-resident queries and results; one captured graph per batch
     d_ip = torch.from_numpy(qs.indptr).to(dev)
     d_ix = torch.from_numpy(qs.indices.view(np.int16)).to(dev)
     d_v = torch.from_numpy(qs.values).to(dev)
     d_D = torch.empty((qs.n, K), dtype=torch.float32, device=dev)
     d_L = torch.empty((qs.n, K), dtype=torch.int32, device=dev)
-    max_nnz = int(np.diff(qs.indptr).max())
     stream = torch.cuda.Stream()
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
-    peak, peak_kind = measured_peaks()
-    tp = nsparse.SeismicSearchParameters(12, 0.9)
-    tp.set_kernel(args.variant, args.tuning)
-    tuned = None
-    if args.variant < 0:
-        sample = qs.rows(0, 4096)
-        tuned = idx.autotune(sample.n, sample.indptr, sample.indices, sample.values, K, tp)
-        log(f"autotune: {tuned}")
-    sweep = []
-    sweep_pairs = SQ_SWEEP if not args.sweep else tuple(
-        (int(c), float(h)) for c, h in (x.split(":") for x in args.sweep.split(",")))
-    for cut, hf in sweep_pairs:
-        params = nsparse.SeismicSearchParameters(cut, hf)
-        params.set_kernel(args.variant, args.tuning)
+    idx.search(64, qs.indptr[:65], qs.indices, qs.values, K, params)  # device images resident
+    bounds = [(b0, min(qs.n, b0 + batch)) for b0 in range(0, qs.n, batch)]
+    # per-batch row pointers rebased to the batch's first entry
+    b_ip = [torch.from_numpy((qs.indptr[b0:b1 + 1] - qs.indptr[b0]).astype(np.int32)).to(dev)
+            for b0, b1 in bounds]
+    graphs = []
+    if not args.no_graph:
+        for (b0, b1), ip in zip(bounds, b_ip):
+            e0 = int(qs.indptr[b0])
+            nnz_b = int(qs.indptr[b1]) - e0
+            mx = int(np.diff(qs.indptr[b0:b1 + 1]).max())
+            graphs.append(nsparse.SearchGraph(
+                idx, b1 - b0, nnz_b, mx, K, params,
+                device_buffers={"indptr": ip.data_ptr(), "indices": d_ix.data_ptr() + 2 * e0,
+                                "values": d_v.data_ptr() + 4 * e0,
+                                "distances": d_D.data_ptr() + 4 * K * b0,
+                                "labels": d_L.data_ptr() + 4 * K * b0}))
+    max_nnz = int(np.diff(qs.indptr).max())
 
-        def one_pass():
-            for b0 in range(0, qs.n, SQ_BATCH):
-                nb = min(SQ_BATCH, qs.n - b0)
-                idx.search_device(nb, d_ip.data_ptr() + 4 * b0, d_ix.data_ptr(), d_v.data_ptr(),
-                                  max_nnz, K, d_D.data_ptr() + 4 * K * b0,
-                                  d_L.data_ptr() + 4 * K * b0, params, stream.cuda_stream)
+    def one_pass():
+        if graphs:
+            for g in graphs:
+                g.launch(stream.cuda_stream)
+        else:
+            for (b0, b1), ip in zip(bounds, b_ip):
+                e0 = int(qs.indptr[b0])
+                idx.search_device(b1 - b0, ip.data_ptr(), d_ix.data_ptr() + 2 * e0,
+                                  d_v.data_ptr() + 4 * e0, max_nnz, K,
+                                  d_D.data_ptr() + 4 * K * b0, d_L.data_ptr() + 4 * K * b0,
+                                  params, stream.cuda_stream)
 
-        idx.search(64, qs.indptr[:65], qs.indices, qs.values, K, params)  # uploads lists
-        with torch.cuda.stream(stream):
-            for _ in range(max(args.warmup, 1)):
-                flush.zero_()
-                one_pass()
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            flush.zero_()
+            one_pass()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with Clocks(torch.cuda.current_device()) as clk, torch.cuda.stream(stream):
+        for i in range(args.steps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            one_pass()
+            ev[i][1].record(stream)
         torch.cuda.synchronize()
-        ev = []
-        with torch.cuda.stream(stream):
-            for _ in range(args.steps):
-                flush.zero_()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                one_pass()
-                e1.record(stream)
-                ev.append((e0, e1))
-        torch.cuda.synchronize()
-        ms = sum(a.elapsed_time(b) for a, b in ev) / len(ev)
-        hD, hL = d_D.cpu().numpy(), d_L.cpu().numpy()
-        # one batch through the host API for the kernel's stats
-        q1 = qs.rows(0, SQ_BATCH)
-        D1, L1 = idx.search(q1.n, q1.indptr, q1.indices, q1.values, K, params)
-        st = nsparse.last_search_stats()
-        assert (L1 == hL[:SQ_BATCH]).all() and (D1 == hD[:SQ_BATCH]).all()
-        plain = nsparse.SeismicSearchParameters(cut, hf)
-        plain.set_kernel(args.variant, args.tuning)
-        plain.set_engine(plain=True)
-        qp = qs.rows(0, SQ_PLAIN)
-        idx.search(4, qp.indptr[:5], qp.indices, qp.values, K, plain)
-        lat = []
-        for q in range(SQ_PLAIN):
-            r1 = qp.rows(q, q + 1)
-            t = time.perf_counter()
-            Dp, Lp = idx.search(1, r1.indptr, r1.indices, r1.values, K, plain)
-            lat.append(time.perf_counter() - t)
-            assert (Lp[0] == hL[q]).all() and (Dp[0] == hD[q]).all()
-        lat_ms = sorted(1000 * x for x in lat)
-        qps = qs.n / (ms / 1000.0)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    for g in graphs:
+        g.sync(stream.cuda_stream)  # raises if the kernel flagged an error
+    hD, hL = d_D.cpu().numpy(), d_L.cpu().numpy()
+    if args.kernel_only:
+        if rank == 0:
+            print(json.dumps({"case": sq_workload(docs, qs, hf, cut),
+                              "variant": args.variant, "tuning": args.tuning,
+                              "ms_per_step": total_ms / args.steps,
+                              "queries_per_s": qs.n * args.steps / (total_ms / 1000.0)}))
+        for g in graphs:
+            g.close()
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+
+    # ---- one batch through the host API: the kernel's own time and its
+    # algorithmic bytes (engine counters), and the same results
+    q1 = qs.rows(0, batch)
+    D1, L1 = idx.search(q1.n, q1.indptr, q1.indices, q1.values, K, params)
+    st = nsparse.last_search_stats()
+    assert (L1 == hL[:batch]).all() and (D1 == hD[:batch]).all(), \
+        "device-resident and host paths disagree"
+
+    # ---- e2e: host buffers through the public API, copies included, the
+    # same 65,536 queries per step in calls of 16,384
+    host_batches = [qs.rows(b0, b1) for b0, b1 in bounds]
+    e2e_t = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        for hb in host_batches:
+            idx.search(hb.n, hb.indptr, hb.indices, hb.values, K, params)
+        e2e_t.append(time.perf_counter() - t)
+    h2d = 4 * (qs.n + len(bounds)) + 6 * qs.nnz
+    d2h = qs.n * K * 8
+
+    # ---- plain: one query per call through the same host API
+    plain = nsparse.SeismicSearchParameters(cut, hf)
+    plain.set_kernel(args.variant, args.tuning)
+    plain.set_engine(plain=True)
+    n_plain = min(SQ_PLAIN, qs.n)
+    qp = qs.rows(0, n_plain)
+    idx.search(4, qp.indptr[:5], qp.indices, qp.values, K, plain)
+    lat = []
+    for q in range(n_plain):
+        r1 = qp.rows(q, q + 1)
+        t = time.perf_counter()
+        Dp, Lp = idx.search(1, r1.indptr, r1.indices, r1.values, K, plain)
+        lat.append(time.perf_counter() - t)
+        assert (Lp[0] == hL[q]).all() and (Dp[0] == hD[q]).all(), "plain and batched disagree"
+    plain_qps = n_plain / sum(lat)
+
+    my_ms, value, e2e_value = replica_throughput(total_ms, sum(e2e_t), qs.n, args.steps,
+                                                 len(e2e_t), world, dev)
+    out = None
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
         achieved = st.bytes / (st.kernel_ms / 1000.0) / 1e9
-        # tie-aware: a returned doc counts if its code score reaches the
-        # exact 10th-best code score (codes tie often)
-        got = hD[:SQ_GT_QUERIES] / decode
-        hit = (got >= Dc[:, K - 1:K] - 0.5) & (hL[:SQ_GT_QUERIES] >= 0)
-        sweep.append({"cut": cut, "heap_factor": hf, "qps": qps, "ms_per_pass": ms,
-                      "recall_at_10": recall_at_k(hL[:SQ_GT_QUERIES], Lt),
-                      "recall_at_10_vs_exact_codes": float(hit.sum() / (SQ_GT_QUERIES * K)),
-                      "plain_qps": SQ_PLAIN / sum(lat), "plain_p50_ms": lat_ms[len(lat_ms) // 2],
-                      "plain_p99_ms": lat_ms[int(0.99 * (len(lat_ms) - 1))],
-                      "batched_over_plain": qps / (SQ_PLAIN / sum(lat)),
-                      "roofline_frac": achieved / peak, "achieved_gbs": achieved,
-                      "docs_scored_per_query": st.docs_scored / q1.n})
-        log(json.dumps(sweep[-1]))
-    # The recall bar is taken against the exact search of the same uint8 codes:
-    # quantising the documents alone caps recall against fp32 scores near
-    # 0.947 on this data, whatever the search does (the sweep keeps both).
-    ok = [s for s in sweep if s["recall_at_10_vs_exact_codes"] >= 0.95]
-    head = (max(ok, key=lambda s: s["qps"]) if ok
-            else max(sweep, key=lambda s: s["recall_at_10_vs_exact_codes"]))
-    # serving at the workload's own query cut (12) and heap factor 0.9
-    serving = [serve_sweep(nsparse, idx, docs, qs, 12, 0.9, args.serve_rates, slots=int(sl))
-               for sl in str(args.serve_slots).split(",")]
-    serving = serving[0] if len(serving) == 1 else serving
-    out = {"metric": "QPS@recall@10>=0.95 vs exact uint8 scores (SEISMIC-SQ, batched, 8.8M docs)",
-           "value": head["qps"], "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
-           "warmup": max(args.warmup, 1), "ms_per_step": head["ms_per_pass"],
-           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
-           "data": "synthetic",
-           "config": {"workload": f"seismic_sq8_{docs.n}_docs_{qs.n}_queries", "docs": docs.n,
-                      "nnz": int(docs.nnz), "queries": qs.n, "batch": SQ_BATCH,
-                      "query_nnz": "uniform 5-200", "lambda": 6000, "beta": 600, "alpha": 0.4,
-                      "cut": head["cut"], "k": K, "heap_factor": head["heap_factor"],
-                      "recall_at_10_vs_exact_codes": head["recall_at_10_vs_exact_codes"],
-                      "recall_at_10_vs_fp32": head["recall_at_10"],
-                      "l2": "flushed between passes; index > L2",
-                      "kernel_variant": args.variant, "kernel_tuning": args.tuning},
-           "build_s": build_s, "autotuned": tuned, "sweep": sweep, "serving": serving,
-           "peak_gbs": peak,
-           "peak_source": peak_kind}
-    print(json.dumps(out))
+        traffic = None
+        prof = os.path.join(ROOT, "profiles", "seismic_search_sq8_8.8M.json")
+        if os.path.exists(prof) and docs.n == SQ_DOCS and batch == SQ_BATCH:
+            try:
+                traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+            except Exception:
+                traffic = None
+        rec = recall_at_k(hL[:n_gt], gt_L)
+        got = hD[:n_gt] / decode
+        hit = (got >= Dc[:, K - 1:K] - 0.5) & (hL[:n_gt] >= 0)
+        lat_ms = sorted(1000 * x for x in lat)
+        out = {
+            "metric": SQ_METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": my_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded; stands in for MS MARCO SPLADE)",
+            "config": dict(sq_workload(docs, qs, hf, cut), parallelism=f"replicas{world}",
+                           step="4 CUDA-graph replays of 16,384 queries" if graphs
+                           else "4 search_device calls of 16,384 queries",
+                           kernel_variant=args.variant, kernel_tuning=args.tuning,
+                           autotuned=tuned),
+            "recall_at_10": rec,
+            "recall_at_10_vs_exact_codes": float(hit.sum() / (n_gt * K)),
+            "recall_queries": n_gt,
+            "build_s": build_s,
+            "plain": {"qps": plain_qps, "queries": n_plain, "api": "Index.search, host buffers",
+                      "p50_ms": lat_ms[len(lat_ms) // 2],
+                      "p99_ms": lat_ms[int(0.99 * (len(lat_ms) - 1))],
+                      "batched_over_plain_same_api": e2e_value / world / plain_qps,
+                      "batched_device_over_plain": value / world / plain_qps},
+            "batch_latency_ms": {"p50": statistics.median(step_ms), "max": max(step_ms)},
+            "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": st.bytes,
+                         "kernel_ms_per_launch": st.kernel_ms,
+                         "launch": f"{batch} queries"},
+            "work": {"docs_scored_per_query": st.docs_scored / q1.n,
+                     "blocks_visited_per_query": st.blocks_visited / q1.n},
+            "gpu_launches": args.steps * (2 * len(graphs) if graphs else len(bounds)),
+            "clocks": clk.summary(),
+        }
+        if world == 1 and not args.no_cpu:
+            with tempfile.TemporaryDirectory() as td:
+                fpath = os.path.join(td, "sq.idx")
+                nsparse.write_index(idx, fpath)
+                cpu, ref = sq_reference_leg(fpath, qs, gt_L, hD, hL, vmin, vmax, cut, hf)
+            out["cpu_baseline"] = cpu
+            out["reference_same_knobs"] = ref
+        if world == 1 and not args.no_serve:
+            out["serving"] = serve_sweep(nsparse, idx, docs, qs, cut, hf, args.serve_rates,
+                                         slots=int(str(args.serve_slots).split(",")[0]))
+    for g in graphs:
+        g.close()
+    if out is not None:
+        print(json.dumps(out))
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def run_reference_sq(args):
+    """The reference arm of the headline: the reference's own build of the
+    8.8M-doc SEISMIC-SQ index (compiled from its sources, oracle/_ref, all host
+    threads), then per step one batched search() of a bounded sample of the
+    same queries at the same knobs. Rank 0 alone runs it."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle as O
+    variant = ref_variant()
+    if variant is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference library not built "
+                                                            "(oracle/_ref)"}))
+        return
+    docs, qs = sq_data(args.docs or SQ_DOCS, 0)
+    if args.queries:
+        qs = qs.rows(0, min(qs.n, args.queries))
+    vmin, vmax = float(docs.values.min()), float(docs.values.max())
+    cores = os.cpu_count()
+    L = O.ref_lib(variant)
+    L.ref_set_threads(cores)
+    t = time.perf_counter()
+    r = O.RefIndex(docs.dim, sq_spec_for(vmin, vmax), variant=variant)
+    r.add(docs)
+    r.build()
+    build_s = time.perf_counter() - t
+    log(f"reference build {build_s:.1f}s on {cores} threads")
+    workload = sq_workload(docs, qs, SQ_HF, SQ_CUT)
+    del docs
+    sample = min(1000, qs.n)  # queries per step: a few seconds of CPU work
+    q = qs.rows(0, sample)
+    for _ in range(args.warmup):
+        r.search(q.rows(0, min(200, sample)), K, param_kind=2, cut=SQ_CUT, heap_factor=SQ_HF)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        r.search(q, K, param_kind=2, cut=SQ_CUT, heap_factor=SQ_HF)
+        times.append(time.perf_counter() - t)
+    value = sample * len(times) / sum(times)
+    lat = _ref_latency(L, r, q, min(200, sample), cores, SQ_CUT, SQ_HF)
+    r.close()
+    print(json.dumps({
+        "metric": SQ_METRIC, "value": value, "unit": "queries/s", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded; stands in for MS MARCO SPLADE)", "impl": "reference",
+        "config": dict(workload, sample_queries=sample,
+                       sample_note=f"each step searches the first {sample} of the {qs.n} "
+                                   "queries (the same query distribution)"),
+        "build_s": build_s,
+        "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cores, "kind": "reference",
+                         "sample": f"{sample} queries per step, one batched search() call, "
+                                   f"reference {variant} build, OMP threads={cores}",
+                         "per_query_1_thread": lat},
+        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}))
 
 
 def run_engine_brutal(args):
@@ -837,15 +1072,17 @@ def serve_sweep(nsparse, idx, docs, qs, cut, hf, rates, seconds=2.0, slots=3):
 
 
 def main():
-    global N_DOCS, N_QUERIES
+    global N_DOCS, N_QUERIES, SQ_CUT, SQ_HF
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--sweep", default="",
-                    help="SEISMIC-SQ (cut:heap_factor) pairs, comma-separated (default: all)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving sweep")
+    ap.add_argument("--cut", type=int, default=None, help="sq8-8.8m: query cut (default 12)")
+    ap.add_argument("--heap-factor", type=float, default=None,
+                    help="sq8-8.8m: heap factor (default 0.9)")
     ap.add_argument("--serve-slots", default="3",
                     help="serving workers (streams); a comma list runs one sweep per value")
     ap.add_argument("--no-graph", action="store_true",
@@ -861,18 +1098,23 @@ def main():
                     help="offered request rates (queries/s) for the serving sweep")
     ap.add_argument("--digest-out", default="",
                     help="build-1m: write one digest per posting list of the device-built file")
-    ap.add_argument("--workload", default="fp32-1m",
-                    choices=["fp32-1m", "sq8-8.8m", "brutal-100k", "build-1m"],
-                    help="fp32-1m: the headline workload; sq8-8.8m: SEISMIC-SQ at 8.8M docs "
-                         "with the serving sweep; brutal-100k: exact brute force; build-1m: "
+    ap.add_argument("--workload", default="sq8-8.8m",
+                    choices=["sq8-8.8m", "fp32-1m", "brutal-100k", "build-1m"],
+                    help="sq8-8.8m (default): SEISMIC-SQ at 8.8M docs, the headline; fp32-1m: "
+                         "SEISMIC fp32 at 1M docs; brutal-100k: exact brute force; build-1m: "
                          "the device build beside the reference's GPU-offload build")
     args = ap.parse_args()
     if args.workload in ("fp32-1m", "build-1m") and (args.docs or args.queries):
         N_DOCS, N_QUERIES = args.docs or N_DOCS, args.queries or N_QUERIES
         WORKLOAD.update(workload=f"seismic_fp32_{N_DOCS}_docs_{N_QUERIES}_queries", docs=N_DOCS,
                         queries=N_QUERIES)
+    SQ_CUT = args.cut if args.cut is not None else SQ_CUT
+    SQ_HF = args.heap_factor if args.heap_factor is not None else SQ_HF
     if args.workload == "sq8-8.8m":
-        run_engine_sq(args)
+        if args.impl == "reference":
+            run_reference_sq(args)
+        else:
+            run_engine_sq(args)
     elif args.workload == "brutal-100k":
         run_engine_brutal(args)
     elif args.workload == "build-1m":

@@ -126,6 +126,20 @@ void nspo_sq_encode_u8(float vmin, float vmax, const float* vals, uint8_t* codes
     }
 }
 
+/* encode_16bit: the same clamp and lround against 65535 (scalar_quantizer.h:108-113). */
+void nspo_sq_encode_u16(float vmin, float vmax, const float* vals, uint16_t* codes,
+                        int64_t n) {
+    const float kmax = 65535.0f;
+    const float range = vmax - vmin;
+    const float inv = kmax / range;
+    for (int64_t i = 0; i < n; ++i) {
+        float scaled = (vals[i] - vmin) * inv;
+        float lo = (scaled < kmax) ? scaled : kmax;
+        float c = (0.0f < lo) ? lo : 0.0f;
+        codes[i] = (uint16_t)lroundf(c);
+    }
+}
+
 float nspo_sq_scale(int qbits, float vmin, float vmax, float qvmin, float qvmax) {
     const float in_range = vmax - vmin;
     const float q_range = qvmax - qvmin;
@@ -135,8 +149,10 @@ float nspo_sq_scale(int qbits, float vmin, float vmax, float qvmin, float qvmax)
 
 /* ---- query cut: utils/vector_process.h:18-30 ---------------------------- */
 
-static inline float val_at(const void* v, int esz, int i) {
-    return esz == 4 ? ((const float*)v)[i] : (float)((const uint8_t*)v)[i];
+static inline float val_at(const void* v, int esz, int64_t i) {
+    if (esz == 4) return ((const float*)v)[i];
+    if (esz == 2) return (float)((const uint16_t*)v)[i];
+    return (float)((const uint8_t*)v)[i];
 }
 
 int nspo_cut(const uint16_t* idx, const void* vals, int esz, int len, int cut,
@@ -200,7 +216,7 @@ int nspo_seismic_search(int dim, int esz, int32_t n_docs, const int32_t* d_indpt
                         const uint16_t* q_indices, const void* q_values, int k,
                         int cut, float heap_factor, const uint64_t* sel_bits,
                         float* out_d, int32_t* out_l, int64_t* stats) {
-    if (k <= 0 || cut <= 0 || dim <= 0 || (esz != 4 && esz != 1)) return -1;
+    if (k <= 0 || cut <= 0 || dim <= 0 || (esz != 4 && esz != 2 && esz != 1)) return -1;
     int64_t max_blocks = 0;
     for (int32_t l = 0; l < n_lists; ++l) {
         int64_t nb = list_block_ptr[l + 1] - list_block_ptr[l];
@@ -211,11 +227,12 @@ int nspo_seismic_search(int dim, int esz, int32_t n_docs, const int32_t* d_indpt
     {
         float* dense = (float*)calloc((size_t)dim, sizeof(float));
         uint8_t* dense8 = (uint8_t*)calloc((size_t)dim, 1);
+        uint16_t* dense16 = (uint16_t*)calloc((size_t)dim, 2);
         uint64_t* visited = (uint64_t*)calloc(((size_t)n_docs + 64) / 64, 8);
         blk_t* blocks = (blk_t*)malloc(sizeof(blk_t) * (size_t)(max_blocks + 1));
         item_t* buf = (item_t*)malloc(sizeof(item_t) * (size_t)k);
         uint16_t* cuts = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)(dim + 1));
-        if (!dense || !dense8 || !visited || !blocks || !buf || !cuts) err = 1;
+        if (!dense || !dense8 || !dense16 || !visited || !blocks || !buf || !cuts) err = 1;
 #pragma omp for schedule(dynamic, 4)
         for (int32_t q = 0; q < n_q; ++q) {
             if (err) continue;
@@ -224,12 +241,16 @@ int nspo_seismic_search(int dim, int esz, int32_t n_docs, const int32_t* d_indpt
             const uint16_t* qi = q_indices + qs;
             const float* qf = esz == 4 ? (const float*)q_values + qs : NULL;
             const uint8_t* q8 = esz == 1 ? (const uint8_t*)q_values + qs : NULL;
+            const uint16_t* q16 = esz == 2 ? (const uint16_t*)q_values + qs : NULL;
+            const void* qany = esz == 4 ? (const void*)qf
+                                        : (esz == 2 ? (const void*)q16 : (const void*)q8);
             /* seismic_index.cpp:244-246: scatter all query terms */
             for (int i = 0; i < qlen; ++i) {
-                if (esz == 4) dense[qi[i]] = qf[i]; else dense8[qi[i]] = q8[i];
+                if (esz == 4) dense[qi[i]] = qf[i];
+                else if (esz == 2) dense16[qi[i]] = q16[i];
+                else dense8[qi[i]] = q8[i];
             }
-            int ncut = nspo_cut(qi, esz == 4 ? (const void*)qf : (const void*)q8,
-                                esz, qlen, cut, cuts);
+            int ncut = nspo_cut(qi, qany, esz, qlen, cut, cuts);
             topk_t h = {buf, 0, k};
             int64_t n_scored = 0, n_blk_visit = 0, n_blk_seen = 0, n_revisit = 0;
             int first = 1;
@@ -250,12 +271,10 @@ int nspo_seismic_search(int dim, int esz, int32_t n_docs, const int32_t* d_indpt
                         for (int i = 0; i < qlen; ++i) {
                             int col = find_term(sum_terms + tp0, ntm, qi[i]);
                             if (col < 0) continue;
-                            const float qv = esz == 4 ? qf[i] : (float)q8[i];
+                            const float qv = val_at(qany, esz, i);
                             for (int64_t j = sum_run_ptr[tp0 + col];
                                  j < sum_run_ptr[tp0 + col + 1]; ++j) {
-                                const float sv =
-                                    esz == 4 ? ((const float*)sum_val)[j]
-                                             : (float)((const uint8_t*)sum_val)[j];
+                                const float sv = val_at(sum_val, esz, j);
                                 const float p = qv * sv;
                                 blocks[sum_block[j]].s = blocks[sum_block[j]].s + p;
                             }
@@ -290,6 +309,13 @@ int nspo_seismic_search(int dim, int esz, int32_t n_docs, const int32_t* d_indpt
                                     float p = dv[e] * dense[d_indices[e]];
                                     s = s + p;
                                 }
+                            } else if (esz == 2) {
+                                /* dot_product_uint16_dense: int64 sum (distance.h:49-57) */
+                                const uint16_t* dv = (const uint16_t*)d_values;
+                                int64_t acc = 0;
+                                for (int32_t e = d_indptr[d]; e < d_indptr[d + 1]; ++e)
+                                    acc += (int64_t)dv[e] * (int64_t)dense16[d_indices[e]];
+                                s = (float)acc;
                             } else {
                                 const uint8_t* dv = (const uint8_t*)d_values;
                                 int acc = 0;
@@ -315,6 +341,7 @@ int nspo_seismic_search(int dim, int esz, int32_t n_docs, const int32_t* d_indpt
             for (int i = 0; i < qlen; ++i) {
                 dense[qi[i]] = 0.0f;
                 dense8[qi[i]] = 0;
+                dense16[qi[i]] = 0;
             }
             for (int c = 0; c < ncut; ++c) {
                 const int t = cuts[c];
@@ -327,6 +354,7 @@ int nspo_seismic_search(int dim, int esz, int32_t n_docs, const int32_t* d_indpt
         }
         free(dense);
         free(dense8);
+        free(dense16);
         free(visited);
         free(blocks);
         free(buf);

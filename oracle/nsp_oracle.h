@@ -47,7 +47,9 @@ int nspo_exact_search(int dim, int32_t n_docs, const int32_t* d_indptr,
  *   to the list.
  * esz = 4: fp32 values/summaries/query; esz = 1: uint8 codes throughout (the
  * query codes are passed in q_codes), scores are int sums cast to float and the
- * caller decodes. `sel_bits` as above. */
+ * caller decodes; esz = 2: uint16 codes, int64 doc sums cast to float
+ * (utils/distance.h:49-57), summary products and sums in float as for every
+ * code width (inverted_list_clusters.cpp:295-315). `sel_bits` as above. */
 int nspo_seismic_search(int dim, int esz, int32_t n_docs, const int32_t* d_indptr,
                         const uint16_t* d_indices, const void* d_values,
                         int32_t n_lists, const int64_t* list_block_ptr,
@@ -62,10 +64,12 @@ int nspo_seismic_search(int dim, int esz, int32_t n_docs, const int32_t* d_indpt
 /* ScalarQuantizer::encode_8bit/16bit (utils/scalar_quantizer.h:97-118). */
 void nspo_sq_encode_u8(float vmin, float vmax, const float* vals, uint8_t* codes,
                        int64_t n);
+void nspo_sq_encode_u16(float vmin, float vmax, const float* vals, uint16_t* codes,
+                        int64_t n);
 /* ScalarQuantizer::decode_dot_product scale (utils/scalar_quantizer.h:85-93). */
 float nspo_sq_scale(int qbits, float vmin, float vmax, float qvmin, float qvmax);
 
-/* Query cut (utils/vector_process.h:18-30) with the tie order above. esz 4 or 1. */
+/* Query cut (utils/vector_process.h:18-30) with the tie order above. esz 4, 2 or 1. */
 int nspo_cut(const uint16_t* idx, const void* vals, int esz, int len, int cut,
              uint16_t* out);
 

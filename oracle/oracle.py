@@ -50,6 +50,8 @@ def lib():
             I32, P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_float, P, P, P, P]
         L.nspo_sq_encode_u8.restype = None
         L.nspo_sq_encode_u8.argtypes = [ctypes.c_float, ctypes.c_float, P, P, I64]
+        L.nspo_sq_encode_u16.restype = None
+        L.nspo_sq_encode_u16.argtypes = [ctypes.c_float, ctypes.c_float, P, P, I64]
         L.nspo_sq_scale.restype = ctypes.c_float
         L.nspo_sq_scale.argtypes = [ctypes.c_int] + [ctypes.c_float] * 4
         L.nspo_cut.restype = ctypes.c_int
@@ -101,8 +103,9 @@ class SeismicArrays:
 def seismic_search(fwd, fwd_values, arrays: SeismicArrays, queries_indptr,
                    queries_indices, queries_values, k, cut, heap_factor,
                    sel_bits=None, want_stats=False):
-    """fwd: Csr-like (dim, n, indptr, indices); fwd_values float32 or uint8 codes;
-    queries_values float32 (esz 4) or uint8 codes (esz 1)."""
+    """fwd: Csr-like (dim, n, indptr, indices); fwd_values float32, uint16 or
+    uint8 codes; queries_values float32 (esz 4), uint16 codes (esz 2) or uint8
+    codes (esz 1)."""
     n_q = len(queries_indptr) - 1
     D = np.empty((n_q, k), dtype=np.float32)
     L = np.empty((n_q, k), dtype=np.int32)
@@ -126,13 +129,20 @@ def sq_encode_u8(vmin, vmax, vals):
     return out
 
 
+def sq_encode_u16(vmin, vmax, vals):
+    vals = np.ascontiguousarray(vals, dtype=np.float32)
+    out = np.empty(len(vals), dtype=np.uint16)
+    lib().nspo_sq_encode_u16(vmin, vmax, _ptr(vals), _ptr(out), len(vals))
+    return out
+
+
 def sq_scale(vmin, vmax, qvmin, qvmax, qbits=8):
     return lib().nspo_sq_scale(qbits, vmin, vmax, qvmin, qvmax)
 
 
 def cut(idx, vals, n_cut):
     idx = np.ascontiguousarray(idx, dtype=np.uint16)
-    esz = 4 if vals.dtype == np.float32 else 1
+    esz = {np.dtype(np.float32): 4, np.dtype(np.uint16): 2}.get(np.dtype(vals.dtype), 1)
     out = np.empty(max(len(idx), n_cut), dtype=np.uint16)
     n = lib().nspo_cut(_ptr(idx), _ptr(vals), esz, len(idx), n_cut, _ptr(out))
     return out[:n]
@@ -370,7 +380,7 @@ def flatten_lists(lists, esz) -> SeismicArrays:
         ltp.append(ltp[-1] + nt)
         blk.append(c["csc_cluster"])
         val.append(c["csc_value"])
-    vdt = np.float32 if esz == 4 else np.uint8
+    vdt = {4: np.float32, 2: np.uint16, 1: np.uint8}[esz]
     cat = lambda xs, dt: np.ascontiguousarray(np.concatenate(xs) if xs else np.zeros(0, dt), dtype=dt)
     return SeismicArrays(
         esz=esz,

@@ -41,9 +41,14 @@ def golden_corpus():
     return docs, qs
 
 
-def sq_spec(vmin, vmax, lam=200, beta=20):
-    return (f"seismic_sq,quantizer=8bit|vmin={float(vmin)!r}|vmax={float(vmax)!r}|"
+def sq_spec(vmin, vmax, lam=200, beta=20, bits=8):
+    return (f"seismic_sq,quantizer={bits}bit|vmin={float(vmin)!r}|vmax={float(vmax)!r}|"
             f"lambda={lam}|beta={beta}|alpha=0.4|seed=7")
+
+
+def sq_codes(vmin, vmax, vals, bits=8):
+    """The reference's ScalarQuantizer::encode (8- or 16-bit), via the oracle."""
+    return (O.sq_encode_u16 if bits == 16 else O.sq_encode_u8)(vmin, vmax, vals)
 
 
 def ref_index(docs, spec, build=True, ids=None):
@@ -93,9 +98,10 @@ def recall(L, T):
     return float(np.mean(vals)) if vals else 1.0
 
 
-def sq_exact_scores(docs, q_codes, qs, labels, vmin, vmax):
-    """Exact integer code dot products (as float32) of each (query, label)."""
-    d_codes = O.sq_encode_u8(vmin, vmax, docs.values)
+def sq_exact_scores(docs, q_codes, qs, labels, vmin, vmax, bits=8):
+    """Exact integer code dot products (as float32) of each (query, label);
+    int64 sums, as the reference sums 16-bit codes (utils/distance.h:49-57)."""
+    d_codes = sq_codes(vmin, vmax, docs.values, bits)
     out = np.zeros(labels.shape, np.float32)
     for q in range(labels.shape[0]):
         qd = np.zeros(docs.dim, np.int64)

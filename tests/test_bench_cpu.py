@@ -15,9 +15,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 @pytest.mark.skipif(not O.ref_available("generic"), reason="reference library not built")
-def test_reference_arm_prints_one_contract_line():
+@pytest.mark.parametrize("workload", ["sq8-8.8m", "fp32-1m"])
+def test_reference_arm_prints_one_contract_line(workload):
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-                        "--docs", "20000", "--queries", "300", "--steps", "2", "--warmup", "1"],
+                        "--workload", workload, "--docs", "20000", "--queries", "300",
+                        "--steps", "2", "--warmup", "1"],
                        capture_output=True, text=True, timeout=600, cwd=ROOT, check=True)
     lines = [ln for ln in r.stdout.splitlines() if ln.strip()]
     assert len(lines) == 1
@@ -27,8 +29,28 @@ def test_reference_arm_prints_one_contract_line():
                 "cpu_baseline", "e2e"):
         assert key in d, key
     assert d["impl"] == "reference" and d["steps"] == 2 and d["value"] > 0
+    assert d["config"]["docs"] == 20000
+    assert d["dtype"] == ("u8" if workload == "sq8-8.8m" else "f32")
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"]
     lat = cb["per_query_1_thread"]
     assert lat["queries"] > 0 and 0 < lat["p50_ms"] <= lat["p99_ms"]
+
+
+def test_row_parity_separates_tied_rows():
+    sys.path.insert(0, ROOT)
+    import numpy as np
+
+    import bench
+    D = np.array([[3.0, 2.0, 1.0], [5.0, 5.0, 4.0], [2.0, 1.0, -1.0]], np.float32)
+    L = np.array([[7, 8, 9], [1, 2, 3], [4, 5, -1]], np.int32)
+    # row 1 is tied (two scores of 5.0): its ids may come in either order
+    Lr = np.array([[7, 8, 9], [2, 1, 3], [4, 5, -1]], np.int32)
+    p = bench.row_parity(D, L, D.copy(), Lr)
+    assert p["rows_identical_frac"] == 2 / 3 and p["rows_same_scores_frac"] == 1.0
+    assert p["untied_rows"] == 2 and p["score_mismatches_untied_rows"] == 0
+    Dr = D.copy()
+    Dr[0, 1] = 2.5
+    p = bench.row_parity(D, L, Dr, Lr)
+    assert p["score_mismatches_untied_rows"] == 1 and p["untied_rows_identical_frac"] == 0.5

@@ -8,7 +8,7 @@ import pytest
 
 import oracle as O
 from helpers import CUT, HF, K, SEISMIC, golden, golden_corpus, oracle_seismic_from_file, \
-    sq_exact_scores, \
+    sq_codes, sq_exact_scores, \
     recall, ref_file, ref_index, sq_spec, unsorted_rows
 from nsparse_b200 import synth
 
@@ -137,6 +137,42 @@ def test_quantizer_matches_reference_encoder():
     want = np.empty(len(vals), np.uint8)
     assert L.ref_sq_encode(8, 0.0158, 84.475, vals.ctypes.data, want.ctypes.data, len(vals)) == 0
     np.testing.assert_array_equal(O.sq_encode_u8(0.0158, 84.475, vals), want)
+
+
+@need_ref
+def test_quantizer_16bit_matches_reference_encoder():
+    L = O.ref_lib("generic")
+    rng = np.random.default_rng(4)
+    vals = np.concatenate([rng.lognormal(0, 0.8, 5000), [-1, 0, 1e9, 0.5]]).astype(np.float32)
+    want = np.empty(len(vals), np.uint16)
+    assert L.ref_sq_encode(16, 0.0158, 84.475, vals.ctypes.data, want.ctypes.data,
+                           len(vals)) == 0
+    np.testing.assert_array_equal(O.sq_encode_u16(0.0158, 84.475, vals), want)
+    # tests/scalar_quantizer_test.cpp (range [0, 1]): ends and midpoint
+    got = O.sq_encode_u16(0.0, 1.0, np.array([0.0, 1.0, 0.5, -0.5, 1.5], np.float32))
+    assert got.tolist() == [0, 65535, 32768, 0, 65535]
+    assert abs(65535.0 * 65535.0 * O.sq_scale(0.0, 1.0, 0.0, 1.0, 16) - 1.0) < 1e-3
+
+
+@need_ref
+def test_seismic_sq16_oracle_matches_reference(tmp_path):
+    """16-bit codes (SeismicScalarQuantizedIndex with quantizer=16bit): the
+    oracle over the reference's own file returns the reference's rows, and
+    every returned score is the exact int64 code sum, decoded."""
+    docs, qs = golden_corpus()
+    vmin, vmax = float(docs.values.min()), float(docs.values.max())
+    r = ref_file(docs, sq_spec(vmin, vmax, bits=16), tmp_path / "q16.idx")
+    assert O.read_index_file(str(tmp_path / "q16.idx"))["vectors"]["esz"] == 2
+    codes = sq_codes(vmin, vmax, qs.values, 16)
+    D, L = oracle_seismic_from_file(tmp_path / "q16.idx", qs, K, CUT, HF, codes=codes)
+    scale = np.float32(O.sq_scale(vmin, vmax, vmin, vmax, 16))
+    Dd = np.where(L >= 0, (D * scale).astype(np.float32), D)
+    Dr, Lr = r.search(qs, K, param_kind=2, cut=CUT, heap_factor=HF)
+    same = (L == Lr).all(axis=1)
+    assert same.mean() >= 0.95
+    np.testing.assert_array_equal(Dd[same], Dr[same])
+    exact = sq_exact_scores(docs, codes, qs, L, vmin, vmax, 16) * scale
+    np.testing.assert_array_equal(Dd[L >= 0], exact[L >= 0])
 
 
 @need_ref

@@ -13,7 +13,7 @@ import pytest
 import nsparse
 import oracle as O
 from helpers import CUT, HF, K, SEISMIC, golden, golden_corpus, oracle_seismic_from_file, recall, \
-    ref_file, sq_exact_scores, sq_spec, unsorted_rows
+    ref_file, sq_codes, sq_exact_scores, sq_spec, unsorted_rows
 from nsparse_b200 import synth
 
 pytestmark = pytest.mark.gpu
@@ -404,6 +404,81 @@ def test_seismic_sq_query_range_override(tmp_path):
     scale = np.float32(O.sq_scale(vmin, vmax, qmin, qmax))
     np.testing.assert_array_equal(L, Lo)
     np.testing.assert_array_equal(D, np.where(Lo >= 0, (Do * scale).astype(np.float32), Do))
+
+
+def _sq16_expect(path, docs, qs, vmin, vmax, qmin, qmax, cut=CUT, hf=HF, k=K):
+    codes = sq_codes(qmin, qmax, qs.values, 16)
+    Do, Lo = oracle_seismic_from_file(path, qs, k, cut, hf, codes=codes)
+    scale = np.float32(O.sq_scale(vmin, vmax, qmin, qmax, 16))
+    return codes, scale, Lo, np.where(Lo >= 0, (Do * scale).astype(np.float32), Do)
+
+
+def test_seismic_sq16_matches_oracle_and_scores_exact(tmp_path):
+    """16-bit codes on the device (uint16 code table, int64 doc sums,
+    scalar_quantizer.h:108-118, distance.h:49-57): ids and scores equal the
+    oracle's, every score is the exact int64 code sum decoded, batched and one
+    query per launch, every kernel variant."""
+    docs, qs = golden_corpus()
+    vmin, vmax = float(docs.values.min()), float(docs.values.max())
+    path = tmp_path / "q16.idx"
+    r = ref_file(docs, sq_spec(vmin, vmax, bits=16), path)
+    idx = nsparse.read_index(str(path))
+    codes, scale, Lo, Do = _sq16_expect(path, docs, qs, vmin, vmax, vmin, vmax)
+    for variant in (-1, 0, 1, 2, 3, 5):
+        p = nsparse.SeismicSearchParameters(CUT, HF)
+        p.set_kernel(variant, 0)
+        D, L = search(idx, qs, params=p)
+        np.testing.assert_array_equal(L, Lo)
+        np.testing.assert_array_equal(D, Do)
+    plain = nsparse.SeismicSearchParameters(CUT, HF)
+    plain.set_engine(plain=True)
+    D, L = search(idx, qs, params=plain)
+    np.testing.assert_array_equal(L, Lo)
+    np.testing.assert_array_equal(D, Do)
+    exact = sq_exact_scores(docs, codes, qs, L, vmin, vmax, 16) * scale
+    np.testing.assert_array_equal(D[L >= 0], exact[L >= 0])
+    # the reference's own search of the same file: the same rows
+    Dr, Lr = r.search(qs, K, param_kind=2, cut=CUT, heap_factor=HF)
+    same = (Lr == L).all(axis=1)
+    assert same.mean() >= 0.95
+    np.testing.assert_array_equal(Dr[same], D[same])
+
+
+def test_seismic_sq16_query_range_and_k100(tmp_path):
+    docs, qs = golden_corpus()
+    vmin, vmax = float(docs.values.min()), float(docs.values.max())
+    path = tmp_path / "q16.idx"
+    ref_file(docs, sq_spec(vmin, vmax, bits=16), path)
+    idx = nsparse.read_index(str(path))
+    qmin, qmax = 0.0, float(qs.values.max())
+    _, _, Lo, Do = _sq16_expect(path, docs, qs, vmin, vmax, qmin, qmax)
+    D, L = search(idx, qs, params=nsparse.SeismicSQSearchParameters(qmin, qmax, CUT, HF))
+    np.testing.assert_array_equal(L, Lo)
+    np.testing.assert_array_equal(D, Do)
+    _, _, Lo, Do = _sq16_expect(path, docs, qs, vmin, vmax, vmin, vmax, k=100)
+    D, L = search(idx, qs, k=100, params=nsparse.SeismicSearchParameters(CUT, HF))
+    np.testing.assert_array_equal(L, Lo)
+    np.testing.assert_array_equal(D, Do)
+
+
+def test_seismic_sq16_device_build(tmp_path):
+    """A 16-bit index built on the device: the file it writes reads back in
+    the reference, and the engine's search of it equals the oracle's."""
+    docs, qs = golden_corpus()
+    vmin, vmax = float(docs.values.min()), float(docs.values.max())
+    idx = make(sq_spec(vmin, vmax, bits=16), docs)
+    path = tmp_path / "dev16.idx"
+    nsparse.write_index(idx, str(path))
+    _, _, Lo, Do = _sq16_expect(path, docs, qs, vmin, vmax, vmin, vmax)
+    D, L = search(idx, qs, params=nsparse.SeismicSearchParameters(CUT, HF))
+    np.testing.assert_array_equal(L, Lo)
+    np.testing.assert_array_equal(D, Do)
+    r = O.RefIndex.read(str(path))
+    Dr, Lr = r.search(qs, K, param_kind=2, cut=CUT, heap_factor=HF)
+    r.close()
+    same = (Lr == L).all(axis=1)
+    assert same.mean() >= 0.95
+    np.testing.assert_array_equal(Dr[same], D[same])
 
 
 def test_idmap_seismic_returns_external_ids(tmp_path):
