@@ -174,10 +174,21 @@ def cpu_baseline(docs, qs, index_file, sample, D_eng=None, L_eng=None, gt_L=None
            "sample": f"{sample} of the {N_QUERIES} queries, one batched search() call, "
                      f"reference {variant} build, OMP threads={cores}",
            "per_query_1_thread": lat}
-    if L_eng is not None:
-        out["parity"] = row_parity(D_eng[:sample], L_eng[:sample], Dr, Lr)
     if gt_L is not None:
-        out["reference_recall_at_10"] = recall_at_k(Lr, gt_L[:sample])
+        out[f"reference_recall_at_10_{variant}"] = recall_at_k(Lr, gt_L[:sample])
+    if L_eng is not None and O.ref_available("generic"):
+        # parity against the reference's generic build: its sequential fp32
+        # sums (utils/distance.h:29-37) are the ones the engine reproduces;
+        # the SIMD builds sum in another order
+        G = O.ref_lib("generic")
+        G.ref_set_threads(cores)
+        g = O.RefIndex.read(index_file, variant="generic")
+        Dg, Lg = g.search(q, K, param_kind=2, cut=CUT, heap_factor=HF)
+        g.close()
+        out["parity"] = dict(row_parity(D_eng[:sample], L_eng[:sample], Dg, Lg),
+                             reference_build="generic (sequential fp32 sums)")
+        if gt_L is not None:
+            out["reference_recall_at_10"] = recall_at_k(Lg, gt_L[:sample])
     return out
 
 
@@ -482,25 +493,71 @@ def sq_workload(docs, qs, hf=SQ_HF, cut=SQ_CUT):
 def row_parity(D, L, Dr, Lr):
     """Engine rows against the reference's rows for the same queries and
     index file. A row is tied when its engine scores repeat a value (the order
-    of equal scores is left unspecified by the reference); on the other rows
-    ids and scores must be identical."""
+    of equal scores is left unspecified by the reference). A doc both return
+    must carry the same score in both (common-pair mismatches); rows may still
+    differ where ties in block scores change the reference's visiting order
+    (its unstable sort, seismic_common.h:105-115), so the overlap of the two
+    result sets is reported too."""
     same = (L == Lr).all(axis=1) & (D == Dr).all(axis=1)
     tied = np.array([len(set(d[l >= 0].tolist())) < int((l >= 0).sum()) for d, l in zip(D, L)])
     same_scores = (np.sort(D, axis=1) == np.sort(Dr, axis=1)).all(axis=1)
     untied = ~tied
     mism = int(((L != Lr) | (D != Dr))[untied].any(axis=1).sum())
+    pairs = pair_mism = 0
+    overlap = []
+    for d, l, dr, lr in zip(D, L, Dr, Lr):
+        ref = {int(i): float(s) for i, s in zip(lr, dr) if i >= 0}
+        mine = {int(i): float(s) for i, s in zip(l, d) if i >= 0}
+        common = ref.keys() & mine.keys()
+        pairs += len(common)
+        pair_mism += sum(1 for i in common if ref[i] != mine[i])
+        if ref:
+            overlap.append(len(common) / len(ref))
     return {"rows": int(len(L)), "rows_identical_frac": float(same.mean()),
             "rows_same_scores_frac": float(same_scores.mean()),
             "untied_rows": int(untied.sum()),
             "untied_rows_identical_frac": float(same[untied].mean()) if untied.any() else 1.0,
-            "score_mismatches_untied_rows": mism}
+            "score_mismatches_untied_rows": mism,
+            "common_pairs": pairs, "common_pair_score_mismatches": pair_mism,
+            "result_overlap": float(np.mean(overlap)) if overlap else 1.0}
 
 
-def sq_reference_leg(index_file, qs, gt_L, D_eng, L_eng, vmin, vmax, cut, hf):
+def sq_exact_check(docs, qs, D, L, vmin, vmax, n):
+    """Every score the engine returned for the first n queries against the
+    exact integer dot product of the uint8 codes (the reference's encode,
+    scalar_quantizer.h:97-101), decoded by the index's scale."""
+    scale = np.float32(255.0) / (np.float32(vmax) - np.float32(vmin))
+
+    def codes(v):
+        x = (v.astype(np.float32) - np.float32(vmin)) * scale
+        return np.floor(np.clip(x, 0, 255) + np.float32(0.5)).astype(np.int64)
+
+    rng_f = np.float32(vmax) - np.float32(vmin)
+    dec = np.float32(rng_f * rng_f) / np.float32(255.0 * 255.0)
+    dense = np.zeros(docs.dim, np.int64)
+    checked = bad = 0
+    for q in range(n):
+        s, e = int(qs.indptr[q]), int(qs.indptr[q + 1])
+        dense[qs.indices[s:e]] = codes(qs.values[s:e])
+        for d, got in zip(L[q], D[q]):
+            if d < 0:
+                continue
+            a, b = int(docs.indptr[d]), int(docs.indptr[d + 1])
+            exact = np.float32(int(np.dot(codes(docs.values[a:b]), dense[docs.indices[a:b]])))
+            checked += 1
+            bad += int(np.float32(exact * dec) != np.float32(got))
+        dense[qs.indices[s:e]] = 0
+    return {"scores_checked": checked, "scores_not_exact": bad}
+
+
+def sq_reference_leg(index_file, qs, gt_L, D_eng, L_eng, cut, hf):
     """The reference's own search (compiled from its sources, oracle/_ref) of
-    the index file the engine wrote: batched QPS on all host threads and
-    per-query single-thread latency (cpu_baseline), its recall@10 at the same
-    (cut, heap factor), and row parity with the engine."""
+    the index file the engine wrote. Its AVX-512 build (the fastest; it sums
+    uint8 products in float): batched QPS on all host threads and per-query
+    single-thread latency (cpu_baseline), and its recall@10 at the same (cut,
+    heap factor). Its generic build (integer sums, as the reference's scalar
+    code defines them): recall and parity with the engine's rows on the recall
+    queries."""
     import oracle as O
     variant = ref_variant()
     if variant is None:
@@ -524,8 +581,19 @@ def sq_reference_leg(index_file, qs, gt_L, D_eng, L_eng, vmin, vmax, cut, hf):
            "sample": f"first {sample} of the {qs.n} queries, one batched search() call on the "
                      f"engine-written index file, reference {variant} build, OMP threads={cores}",
            "index_read_s": read_s, "per_query_1_thread": lat}
-    ref = {"recall_at_10": recall_at_k(Lr[:n_gt], gt_L),
-           "parity": row_parity(D_eng[:sample], L_eng[:sample], Dr, Lr)}
+    ref = {f"recall_at_10_{variant}": recall_at_k(Lr[:n_gt], gt_L)}
+    if O.ref_available("generic"):
+        G = O.ref_lib("generic")
+        G.ref_set_threads(cores)
+        g = O.RefIndex.read(index_file, variant="generic")
+        qg = qs.rows(0, n_gt)
+        Dg, Lg = g.search(qg, K, param_kind=2, cut=cut, heap_factor=hf)
+        g.close()
+        ref["recall_at_10"] = recall_at_k(Lg, gt_L)
+        ref["parity"] = dict(row_parity(D_eng[:n_gt], L_eng[:n_gt], Dg, Lg),
+                             reference_build="generic (integer code sums)")
+    else:
+        ref["recall_at_10"] = ref[f"recall_at_10_{variant}"]
     return cpu, ref
 
 
@@ -764,6 +832,7 @@ def run_engine_sq(args):
             "recall_at_10": rec,
             "recall_at_10_vs_exact_codes": float(hit.sum() / (n_gt * K)),
             "recall_queries": n_gt,
+            "exact_scores": sq_exact_check(docs, qs, hD, hL, vmin, vmax, min(200, n_gt)),
             "build_s": build_s,
             "plain": {"qps": plain_qps, "queries": n_plain, "api": "Index.search, host buffers",
                       "p50_ms": lat_ms[len(lat_ms) // 2],
@@ -787,7 +856,7 @@ def run_engine_sq(args):
             with tempfile.TemporaryDirectory() as td:
                 fpath = os.path.join(td, "sq.idx")
                 nsparse.write_index(idx, fpath)
-                cpu, ref = sq_reference_leg(fpath, qs, gt_L, hD, hL, vmin, vmax, cut, hf)
+                cpu, ref = sq_reference_leg(fpath, qs, gt_L, hD, hL, cut, hf)
             out["cpu_baseline"] = cpu
             out["reference_same_knobs"] = ref
         if world == 1 and not args.no_serve:

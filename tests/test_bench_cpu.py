@@ -54,3 +54,33 @@ def test_row_parity_separates_tied_rows():
     Dr[0, 1] = 2.5
     p = bench.row_parity(D, L, Dr, Lr)
     assert p["score_mismatches_untied_rows"] == 1 and p["untied_rows_identical_frac"] == 0.5
+
+
+def test_exact_score_check_flags_a_wrong_score():
+    sys.path.insert(0, ROOT)
+    import numpy as np
+
+    import bench
+    from nsparse_b200 import synth
+    docs = synth.docs_config2(1500, seed=0)
+    qs = synth.queries_config2(12, seed=1)
+    vmin, vmax = float(docs.values.min()), float(docs.values.max())
+    dc = O.sq_encode_u8(vmin, vmax, docs.values).astype(np.int64)
+    qc = O.sq_encode_u8(vmin, vmax, qs.values).astype(np.int64)
+    rng = np.float32(vmax) - np.float32(vmin)
+    dec = np.float32(rng * rng) / np.float32(255.0 * 255.0)
+    D = np.zeros((qs.n, 10), np.float32)
+    L = np.zeros((qs.n, 10), np.int32)
+    for q in range(qs.n):
+        dense = np.zeros(docs.dim, np.int64)
+        s, e = qs.indptr[q], qs.indptr[q + 1]
+        dense[qs.indices[s:e]] = qc[s:e]
+        sc = np.array([int(np.dot(dc[docs.indptr[d]:docs.indptr[d + 1]],
+                                  dense[docs.indices[docs.indptr[d]:docs.indptr[d + 1]]]))
+                       for d in range(docs.n)])
+        o = np.lexsort((np.arange(docs.n), -sc))[:10]
+        L[q], D[q] = o, (sc[o].astype(np.float32) * dec).astype(np.float32)
+    assert bench.sq_exact_check(docs, qs, D, L, vmin, vmax, qs.n) == \
+        {"scores_checked": 10 * qs.n, "scores_not_exact": 0}
+    D[3, 2] = np.nextafter(D[3, 2], np.float32(np.inf))
+    assert bench.sq_exact_check(docs, qs, D, L, vmin, vmax, qs.n)["scores_not_exact"] == 1
