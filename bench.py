@@ -118,6 +118,16 @@ class Clocks:
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(self.rows)}
 
 
+def reference_inputs():
+    """The reference arm generates its inputs with the oracle's build of the
+    corpus generator (the same C source), so it maps no library of the
+    engine's tree."""
+    from nsparse_b200 import synth
+    p = os.path.join(ROOT, "oracle", "_bin", "libnsp_synth.so")
+    if os.path.exists(p):
+        synth.use_library(p)
+
+
 def make_data(rank):
     from nsparse_b200 import synth
     docs = synth.docs_config0(N_DOCS, seed=0)
@@ -228,6 +238,7 @@ def run_reference(args):
     if variant is None:
         print(json.dumps({"impl": "reference", "unavailable": "reference library not built (oracle/_ref)"}))
         return
+    reference_inputs()
     docs, qs = make_data(0)
     cores = os.cpu_count()
     O.ref_lib(variant).ref_set_threads(cores)
@@ -289,8 +300,10 @@ def run_engine(args):
     params.set_kernel(args.variant, args.tuning)
     tuned = None
     if args.variant < 0:
-        # the engine's autotuner picks the launch shape on a 2,000-query sample
-        sample = qs.rows(0, min(qs.n, 2000))
+        # the engine's autotuner picks the launch shape on 2,000 queries drawn
+        # apart from the timed ones (seed 999; the timed queries use 1000+)
+        from nsparse_b200 import synth
+        sample = synth.queries_config0(2000, seed=999)
         tuned = idx.autotune(sample.n, sample.indptr, sample.indices, sample.values, K, params)
         log(f"autotune: {tuned}")
 
@@ -885,6 +898,7 @@ def run_reference_sq(args):
         print(json.dumps({"impl": "reference", "unavailable": "reference library not built "
                                                             "(oracle/_ref)"}))
         return
+    reference_inputs()
     docs, qs = sq_data(args.docs or SQ_DOCS, 0)
     if args.queries:
         qs = qs.rows(0, min(qs.n, args.queries))

@@ -1,7 +1,8 @@
 """Builds the engine's shared libraries in-tree (they travel with the repo).
 
-  lib/libnsparse_b200.so  CUDA kernels (sm_100a) + C++ API + C ABI
-  lib/libnsp_synth.so     seeded synthetic corpus generator (plain C)
+  lib/libnsparse_b200.so    CUDA kernels (sm_100a) + C++ API + C ABI
+  synth/libnsp_synth.so     seeded synthetic corpus generator (plain C; the
+                            benchmark's and tests' input data, not the engine)
 
 Usage: python neural-sparse-cpp_b200/build.py [--force]
 """
@@ -90,9 +91,9 @@ def build_engine(force=False, jobs=8):
 def build_synth(force=False):
     os.makedirs(OBJ, exist_ok=True)
     src = os.path.join(HERE, "synth", "nsp_synth.c")
-    so = os.path.join(LIB, "libnsp_synth.so")
+    so = os.path.join(HERE, "synth", "libnsp_synth.so")
     if force or _stale(so, [src]):
-        obj = os.path.join(OBJ, "nsp_synth.o")
+        obj = os.path.join(HERE, "synth", "nsp_synth.o")
         gomp = next((p for p in LIBGOMP_CANDIDATES if os.path.exists(p)), "-lgomp")
         _run(["gcc", "-std=c11", "-O2", "-fPIC", "-fopenmp", "-c", src, "-o", obj])
         _run(["gcc", "-shared", "-o", so, obj, gomp, "-lm"])

@@ -1,8 +1,8 @@
 """Seeded synthetic sparse corpora standing in for MS MARCO SPLADE vectors.
 
 The generator itself is C (``synth/nsp_synth.c``, built into
-``lib/libnsp_synth.so``); this module sizes the buffers and names the workload
-shapes used by the benchmarks and tests:
+``synth/libnsp_synth.so``, apart from the engine library); this module sizes
+the buffers and names the workload shapes used by the benchmarks and tests:
 
 * ``docs_config0`` -- doc nnz lognormal(median 110, sigma 0.6) clipped to
   [10, 400]; Zipf(1.1) terms over the 30,522-term vocabulary without
@@ -24,14 +24,23 @@ import numpy as np
 VOCAB = 30522
 
 _LIB = None
+_PATH = os.path.abspath(os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "..",
+                                     "synth", "libnsp_synth.so"))
+
+
+def use_library(path: str) -> None:
+    """Loads the generator from `path` (the same C source built elsewhere)
+    instead of the package's own build; call before the first corpus."""
+    global _PATH
+    if _LIB is not None:
+        raise RuntimeError("the generator library is already loaded")
+    _PATH = os.path.abspath(path)
 
 
 def _lib():
     global _LIB
     if _LIB is None:
-        here = os.path.dirname(os.path.abspath(__file__))
-        path = os.path.join(here, "..", "..", "lib", "libnsp_synth.so")
-        lib = ctypes.CDLL(os.path.abspath(path))
+        lib = ctypes.CDLL(_PATH)
         lib.nsp_synth_indptr.restype = ctypes.c_int64
         lib.nsp_synth_indptr.argtypes = [
             ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int,

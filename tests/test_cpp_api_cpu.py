@@ -16,7 +16,7 @@ import pytest
 import oracle as O
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REFERENCE = "/root/reference"
+REFERENCE = os.environ.get("NSP_REFERENCE_DIR", "/root/reference")
 
 CLIENT = r"""
 #include <cstdint>
