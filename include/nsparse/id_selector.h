@@ -6,6 +6,7 @@
 #define NSPARSE_B200_ID_SELECTOR_H
 
 #include <algorithm>
+#include <climits>
 #include <cstddef>
 #include <cstdint>
 #include <unordered_set>
@@ -19,6 +20,12 @@ class IDSelector {
 public:
     virtual ~IDSelector() = default;
     virtual bool is_member(idx_t id) const = 0;
+    // Extension: membership of a 64-bit id (an IDMapIndex's external ids).
+    // The default answers is_member for ids that fit 32 bits and false
+    // otherwise.
+    virtual bool is_member64(int64_t id) const {
+        return id >= INT32_MIN && id <= INT32_MAX && is_member(static_cast<idx_t>(id));
+    }
     bool operator()(idx_t id) const { return is_member(id); }
     // Sets bit d of `bits` (n_docs bits, zero on entry) for every member d in
     // [0, n_docs). The default asks is_member for every id.
@@ -35,6 +42,11 @@ public:
         return v;
     }
     virtual size_t size() const = 0;
+    // Extension: the ids at 64 bits (the default widens ids()).
+    virtual std::vector<int64_t> ids64() const {
+        const std::vector<idx_t> v = ids();
+        return {v.begin(), v.end()};
+    }
     void fill_bitmap(uint64_t* bits, int64_t n_docs) const override;
 };
 
@@ -72,6 +84,26 @@ public:
 
 private:
     IDSelector* delegate_;
+};
+
+// Extension: a set of 64-bit ids, for an IDMapIndex whose external ids need
+// them. ids() lists the members that fit 32 bits; size() counts them all.
+class SetIDSelector64 : public IDSelectorEnumerable {
+public:
+    SetIDSelector64(size_t n, const int64_t* indices) : ids_(indices, indices + n) {}
+    bool is_member(idx_t id) const override { return ids_.count(id) != 0; }
+    bool is_member64(int64_t id) const override { return ids_.count(id) != 0; }
+    std::vector<idx_t> ids() const override {
+        std::vector<idx_t> out;
+        for (int64_t v : ids_)
+            if (v >= INT32_MIN && v <= INT32_MAX) out.push_back(static_cast<idx_t>(v));
+        return out;
+    }
+    std::vector<int64_t> ids64() const override { return {ids_.begin(), ids_.end()}; }
+    size_t size() const override { return ids_.size(); }
+
+private:
+    std::unordered_set<int64_t> ids_;
 };
 
 // Extension: a ready-made membership bitmap over ids [0, n_bits) (bit d of

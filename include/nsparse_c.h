@@ -59,6 +59,13 @@ nsp_status_t nsp_index_add_with_ids(nsp_index_t* index, int32_t n, const int32_t
                                     const uint16_t* indices, const float* values,
                                     const int32_t* ids);
 
+/* Extension with no counterpart in the reference (whose ids are 32 bits):
+ * IDMapIndex::add_with_ids with 64-bit external ids. Other index types raise
+ * as add_with_ids does. */
+nsp_status_t nsp_index_add_with_ids64(nsp_index_t* index, int32_t n, const int32_t* indptr,
+                                      const uint16_t* indices, const float* values,
+                                      const int64_t* ids);
+
 /* Index::build (nsparse/index.h:36). SEISMIC indexes build on the GPU. */
 nsp_status_t nsp_index_build(nsp_index_t* index);
 
@@ -70,6 +77,15 @@ nsp_status_t nsp_index_search(nsp_index_t* index, int32_t n, const int32_t* indp
                               const uint16_t* indices, const float* values, int k,
                               float* distances, int32_t* labels,
                               const nsp_search_params_t* params);
+
+/* Extension with no counterpart in the reference: nsp_index_search with
+ * 64-bit labels, for an IDMapIndex whose external ids need them (its
+ * nsp_index_search raises NSP_ERR_INVALID_ARGUMENT once one does). Other
+ * index types return their 32-bit labels widened. */
+nsp_status_t nsp_index_search64(nsp_index_t* index, int32_t n, const int32_t* indptr,
+                                const uint16_t* indices, const float* values, int k,
+                                float* distances, int64_t* labels,
+                                const nsp_search_params_t* params);
 
 /* Index::num_vectors (nsparse/index.h:45-48). */
 nsp_status_t nsp_index_num_vectors(const nsp_index_t* index, int64_t* out);
@@ -107,6 +123,9 @@ nsp_status_t nsp_id_selector_not_new(nsp_id_selector_t* inner, nsp_id_selector_t
  * bitmap over ids [0, n_bits), bit d of word d/64; the bits are copied. */
 nsp_status_t nsp_id_selector_bitmap_new(int64_t n_bits, const uint64_t* bits,
                                         nsp_id_selector_t** out);
+/* Extension with no counterpart in the reference: a set of 64-bit ids (an
+ * IDMapIndex's wide external ids). */
+nsp_status_t nsp_id_selector_set64_new(size_t n, const int64_t* ids, nsp_id_selector_t** out);
 nsp_status_t nsp_id_selector_is_member(const nsp_id_selector_t* sel, int32_t id, int* out);
 nsp_status_t nsp_id_selector_free(nsp_id_selector_t* sel);
 

@@ -101,6 +101,22 @@ nsp_status_t nsp_index_add_with_ids(nsp_index_t* index, int32_t n, const int32_t
     return guarded([&] { as_index(index)->add_with_ids(n, indptr, indices, values, ids); });
 }
 
+nsp_status_t nsp_index_add_with_ids64(nsp_index_t* index, int32_t n, const int32_t* indptr,
+                                      const uint16_t* indices, const float* values,
+                                      const int64_t* ids) {
+    return guarded([&] {
+        Index* idx = as_index(index);
+        if (auto* m = dynamic_cast<IDMapIndex*>(idx)) {
+            m->add_with_ids64(n, indptr, indices, values, ids);
+            return;
+        }
+        // the base's behaviour for an index without an id map
+        if (n > 0 && ids == nullptr) throw std::invalid_argument("unexpected nullptr");
+        std::vector<idx_t> narrow(ids, ids + (n > 0 ? n : 0));
+        idx->add_with_ids(n, indptr, indices, values, narrow.data());
+    });
+}
+
 nsp_status_t nsp_index_build(nsp_index_t* index) {
     return guarded([&] { as_index(index)->build(); });
 }
@@ -112,6 +128,24 @@ nsp_status_t nsp_index_search(nsp_index_t* index, int32_t n, const int32_t* indp
     return guarded([&] {
         as_index(index)->search(n, indptr, indices, values, k, distances, labels,
                                 as_params(params));
+    });
+}
+
+nsp_status_t nsp_index_search64(nsp_index_t* index, int32_t n, const int32_t* indptr,
+                                const uint16_t* indices, const float* values, int k,
+                                float* distances, int64_t* labels,
+                                const nsp_search_params_t* params) {
+    return guarded([&] {
+        Index* idx = as_index(index);
+        if (auto* m = dynamic_cast<IDMapIndex*>(idx)) {
+            m->search64(n, indptr, indices, values, k, distances, labels, as_params(params));
+            return;
+        }
+        if (labels == nullptr) throw std::invalid_argument("unexpected nullptr");
+        std::vector<idx_t> narrow(n > 0 && k > 0 ? static_cast<size_t>(n) * k : 0);
+        idx->search(n, indptr, indices, values, k, distances, narrow.empty() ? nullptr : narrow.data(),
+                    as_params(params));
+        for (size_t i = 0; i < narrow.size(); ++i) labels[i] = narrow[i];
     });
 }
 
@@ -167,6 +201,14 @@ nsp_status_t nsp_id_selector_set_new(size_t n, const int32_t* ids, nsp_id_select
         check_out(out);
         if (n > 0 && ids == nullptr) throw std::invalid_argument("unexpected nullptr");
         *out = reinterpret_cast<nsp_id_selector_t*>(new SetIDSelector(n, ids));
+    });
+}
+
+nsp_status_t nsp_id_selector_set64_new(size_t n, const int64_t* ids, nsp_id_selector_t** out) {
+    return guarded([&] {
+        check_out(out);
+        if (n > 0 && ids == nullptr) throw std::invalid_argument("unexpected nullptr");
+        *out = reinterpret_cast<nsp_id_selector_t*>(new SetIDSelector64(n, ids));
     });
 }
 

@@ -138,10 +138,10 @@ std::vector<uint64_t> selector_bitmap(const IDSelector* sel, int64_t n_docs) {
 // is_member and ids() translate between internal and external ids.
 class IDSelectorWithIDMap : public IDSelector {
 public:
-    IDSelectorWithIDMap(const IDSelector* d, const std::vector<idx_t>& map,
-                        const std::unordered_map<idx_t, idx_t>& ext)
+    IDSelectorWithIDMap(const IDSelector* d, const std::vector<int64_t>& map,
+                        const std::unordered_map<int64_t, idx_t>& ext)
         : delegate_(d), map_(map), ext_(ext) {}
-    bool is_member(idx_t id) const override { return delegate_->is_member(map_[id]); }
+    bool is_member(idx_t id) const override { return delegate_->is_member64(map_[id]); }
     void fill_bitmap(uint64_t* bits, int64_t n_docs) const override {
         // NOT(enumerable): everything but the mapped ids of the inner set.
         if (const auto* nots = dynamic_cast<const NotIDSelector*>(delegate_)) {
@@ -149,7 +149,7 @@ public:
                 const int64_t words = (n_docs + 63) / 64;
                 for (int64_t w = 0; w < words; ++w) bits[w] = ~uint64_t{0};
                 if (n_docs % 64 != 0) bits[words - 1] = (uint64_t{1} << (n_docs % 64)) - 1;
-                for (idx_t e : en->ids()) {
+                for (int64_t e : en->ids64()) {
                     auto it = ext_.find(e);
                     if (it != ext_.end() && it->second < n_docs)
                         bits[it->second >> 6] &= ~(uint64_t{1} << (it->second & 63));
@@ -159,24 +159,26 @@ public:
         }
         const int64_t m = std::min<int64_t>(n_docs, static_cast<int64_t>(map_.size()));
         for (int64_t d = 0; d < m; ++d)
-            if (delegate_->is_member(map_[d])) set_bit(bits, d);
+            if (delegate_->is_member64(map_[d])) set_bit(bits, d);
     }
 
 private:
     const IDSelector* delegate_;
-    const std::vector<idx_t>& map_;
-    const std::unordered_map<idx_t, idx_t>& ext_;
+    const std::vector<int64_t>& map_;
+    const std::unordered_map<int64_t, idx_t>& ext_;
 };
 
+// id_map_index.h:42-75: an enumerable external selector enumerates the
+// internal ids of its members.
 class IDSelectorEnumerableWithIDMap : public IDSelectorEnumerable {
 public:
-    IDSelectorEnumerableWithIDMap(const IDSelectorEnumerable* d, const std::vector<idx_t>& map,
-                                  const std::unordered_map<idx_t, idx_t>& ext)
+    IDSelectorEnumerableWithIDMap(const IDSelectorEnumerable* d, const std::vector<int64_t>& map,
+                                  const std::unordered_map<int64_t, idx_t>& ext)
         : delegate_(d), map_(map), ext_(ext) {}
-    bool is_member(idx_t id) const override { return delegate_->is_member(map_[id]); }
+    bool is_member(idx_t id) const override { return delegate_->is_member64(map_[id]); }
     std::vector<idx_t> ids() const override {
         std::vector<idx_t> out;
-        for (idx_t e : delegate_->ids()) {
+        for (int64_t e : delegate_->ids64()) {
             auto it = ext_.find(e);
             if (it != ext_.end()) out.push_back(it->second);
         }
@@ -188,8 +190,8 @@ public:
 
 private:
     const IDSelectorEnumerable* delegate_;
-    const std::vector<idx_t>& map_;
-    const std::unordered_map<idx_t, idx_t>& ext_;
+    const std::vector<int64_t>& map_;
+    const std::unordered_map<int64_t, idx_t>& ext_;
 };
 
 // ---------------------------------------------------------- state types --
@@ -804,17 +806,32 @@ void IDMapIndex::add_with_ids(idx_t n, const idx_t* indptr, const term_t* indice
                               const float* values, const idx_t* ids) {
     const size_t old = delegate_->num_vectors();
     delegate_->add(n, indptr, indices, values);
-    internal_to_external_.resize(old + n);
+    std::vector<int64_t> wide(ids, ids + (n > 0 ? n : 0));
+    map_ids(old, n, wide.data());
+}
+
+void IDMapIndex::add_with_ids64(idx_t n, const idx_t* indptr, const term_t* indices,
+                                const float* values, const int64_t* ids) {
+    if (n > 0 && ids == nullptr) throw std::invalid_argument("unexpected nullptr");
+    const size_t old = delegate_->num_vectors();
+    delegate_->add(n, indptr, indices, values);
+    map_ids(old, n, ids);
+}
+
+void IDMapIndex::map_ids(size_t first, idx_t n, const int64_t* ids) {
+    internal_to_external_.resize(first + (n > 0 ? n : 0));
     for (idx_t i = 0; i < n; ++i) {
-        internal_to_external_[old + i] = ids[i];
-        external_to_internal_[ids[i]] = static_cast<idx_t>(old + i);
+        internal_to_external_[first + i] = ids[i];
+        external_to_internal_[ids[i]] = static_cast<idx_t>(first + i);
+        wide_ = wide_ || ids[i] < INT32_MIN || ids[i] > INT32_MAX;
     }
 }
 
 // id_map_index.cpp:29-60. The caller's selector is restored on return (the
 // reference leaves the translated one in place).
-void IDMapIndex::search(idx_t n, const idx_t* indptr, const term_t* indices, const float* values,
-                        int k, float* distances, idx_t* labels, SearchParameters* params) {
+void IDMapIndex::search_internal(idx_t n, const idx_t* indptr, const term_t* indices,
+                                 const float* values, int k, float* distances, idx_t* labels,
+                                 SearchParameters* params) {
     std::unique_ptr<IDSelector> wrapped;
     IDSelector* original = nullptr;
     if (params != nullptr && params->get_id_selector() != nullptr) {
@@ -835,10 +852,32 @@ void IDMapIndex::search(idx_t n, const idx_t* indptr, const term_t* indices, con
         throw;
     }
     if (original != nullptr) params->set_id_selector(original);
+}
+
+void IDMapIndex::search(idx_t n, const idx_t* indptr, const term_t* indices, const float* values,
+                        int k, float* distances, idx_t* labels, SearchParameters* params) {
+    if (wide_)
+        throw std::invalid_argument(
+            "external ids need 64 bits: search with search64 (32-bit labels cannot hold them)");
+    search_internal(n, indptr, indices, values, k, distances, labels, params);
     const size_t cnt = static_cast<size_t>(n) * k;
     for (size_t i = 0; i < cnt; ++i) {
-        if (labels[i] >= 0) labels[i] = internal_to_external_[labels[i]];
+        if (labels[i] >= 0) labels[i] = static_cast<idx_t>(internal_to_external_[labels[i]]);
     }
+}
+
+void IDMapIndex::search64(idx_t n, const idx_t* indptr, const term_t* indices, const float* values,
+                          int k, float* distances, int64_t* labels, SearchParameters* params) {
+    if (labels == nullptr) throw std::invalid_argument("unexpected nullptr");
+    if (n <= 0 || k <= 0) {
+        // the delegate raises the reference's argument errors
+        search_internal(n, indptr, indices, values, k, distances, nullptr, params);
+        return;
+    }
+    std::vector<idx_t> internal(static_cast<size_t>(n) * k);
+    search_internal(n, indptr, indices, values, k, distances, internal.data(), params);
+    for (size_t i = 0; i < internal.size(); ++i)
+        labels[i] = internal[i] >= 0 ? internal_to_external_[internal[i]] : -1;
 }
 
 // ------------------------------------------------------------ factory ----

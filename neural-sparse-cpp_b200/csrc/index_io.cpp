@@ -418,10 +418,18 @@ void InvertedIndex::read_index(IOReader* r, int) {
     built_ = n_terms > 0;
 }
 
+// The reference's IDMP layout (id_map_index.cpp:82-99): the id count, then
+// 32-bit ids. A map with ids beyond 32 bits is written under the name64 tag
+// with 64-bit ids (engine extension).
 void IDMapIndex::write_index(IOWriter* w) {
     write_scalar<size_t>(w, internal_to_external_.size());
-    if (!internal_to_external_.empty())
-        w->write(internal_to_external_.data(), sizeof(idx_t), internal_to_external_.size());
+    if (wide_) {
+        if (!internal_to_external_.empty())
+            w->write(internal_to_external_.data(), sizeof(int64_t), internal_to_external_.size());
+    } else {
+        std::vector<idx_t> narrow(internal_to_external_.begin(), internal_to_external_.end());
+        if (!narrow.empty()) w->write(narrow.data(), sizeof(idx_t), narrow.size());
+    }
     nsparse::write_index(delegate_.get(), w);
 }
 
@@ -429,12 +437,22 @@ namespace detail {
 Index* read_index_nested(IOReader* r, int io_flags);
 }
 
-void IDMapIndex::read_index(IOReader* r, int io_flags) {
+void IDMapIndex::read_index(IOReader* r, int io_flags, bool wide) {
     const size_t m = read_scalar<size_t>(r);
-    internal_to_external_ = read_padded<idx_t>(r, m, 1);
+    if (wide) {
+        internal_to_external_ = read_padded<int64_t>(r, m, 1);
+    } else {
+        const std::vector<idx_t> narrow = read_padded<idx_t>(r, m, 1);
+        internal_to_external_.assign(narrow.begin(), narrow.end());
+    }
     delegate_.reset(detail::read_index_nested(r, io_flags));
     external_to_internal_.clear();
-    for (size_t i = 0; i < m; ++i) external_to_internal_[internal_to_external_[i]] = static_cast<idx_t>(i);
+    wide_ = false;
+    for (size_t i = 0; i < m; ++i) {
+        const int64_t e = internal_to_external_[i];
+        external_to_internal_[e] = static_cast<idx_t>(i);
+        wide_ = wide_ || e < INT32_MIN || e > INT32_MAX;
+    }
 }
 
 // ------------------------------------------------------------ free API --
@@ -453,7 +471,8 @@ void write_index(Index* index, IOWriter* w) {
         header();
         q->write_index(w);
     } else if (auto* m = dynamic_cast<IDMapIndex*>(index)) {
-        header();
+        write_scalar<uint32_t>(w, m->wide_ids() ? fourcc(IDMapIndex::name64) : id);
+        write_scalar<int32_t>(w, index->get_dimension());
         m->write_index(w);
     } else if (auto* v = dynamic_cast<InvertedIndex*>(index)) {
         header();
@@ -489,10 +508,10 @@ Index* read_index_nested(IOReader* r, int io_flags) {
         auto* p = new SeismicScalarQuantizedIndex(dim);
         idx.reset(p);
         p->read_index(r, io_flags);
-    } else if (id == fourcc(IDMapIndex::name)) {
+    } else if (id == fourcc(IDMapIndex::name) || id == fourcc(IDMapIndex::name64)) {
         auto* p = new IDMapIndex();
         idx.reset(p);
-        p->read_index(r, io_flags);
+        p->read_index(r, io_flags, id == fourcc(IDMapIndex::name64));
     } else if (id == fourcc(InvertedIndex::name)) {
         auto* p = new InvertedIndex(dim);
         idx.reset(p);

@@ -70,15 +70,16 @@ struct Seg {
     int32_t blk;    // block index within its list
     float bs;       // the block's summary score
     int32_t head;   // 1 when the block starts here (its pruning test applies)
-    int32_t pad;
+    int32_t surv;   // docs that may still enter the heap (counted after scoring)
 };
 
 struct Ctl {
     int32_t q;
     int32_t nseg;
     int32_t total;
-    int32_t next;  // claim counter of the scoring phase
-    int32_t pad[4];
+    int32_t next;   // claim counter of the scoring phase
+    int32_t nheap;  // heap size when the batch was gathered (warp 0's)
+    int32_t pad[3];
 };
 
 __host__ __device__ inline size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
@@ -164,8 +165,20 @@ __device__ __forceinline__ void products(const uint16_t* ip, const float* vp, in
     }
 }
 
+// The query codes of row terms u0..u0+3, packed one byte each (byte j = the
+// code of term u0+j) so that one __dp4a multiplies them with the four doc
+// codes a values word holds and adds the four products.
+template <typename TE>
+__device__ __forceinline__ uint32_t codes4(const uint32_t (&t)[8], int u0, const TE* tbl) {
+    const uint32_t q0 = tbl[term_of(t, u0)];
+    const uint32_t q1 = tbl[term_of(t, u0 + 1)];
+    const uint32_t q2 = tbl[term_of(t, u0 + 2)];
+    const uint32_t q3 = tbl[term_of(t, u0 + 3)];
+    return __byte_perm(__byte_perm(q0, q1, 0x3240), __byte_perm(q2, q3, 0x3240), 0x5410);
+}
+
 // uint8 codes: the sum of code products as int (distance.h:39-47); padding
-// codes are 0.
+// codes are 0. Sums of at most 2^16 products of two codes stay below 2^32.
 template <typename TE>
 __device__ __forceinline__ int partial(const uint16_t* ip, const uint8_t* vp, int rem,
                                        const TE* tbl) {
@@ -174,14 +187,10 @@ __device__ __forceinline__ int partial(const uint16_t* ip, const uint8_t* vp, in
     ldg256(ip, t);
     const uint4 v = __ldg(reinterpret_cast<const uint4*>(vp));
     const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-    int acc = 0;
+    uint32_t acc = 0;
 #pragma unroll
-    for (int u = 0; u < 16; ++u) {
-        const int q = static_cast<int>(tbl[term_of(t, u)]);
-        const int x = static_cast<int>((w[u >> 2] >> (8 * (u & 3))) & 0xffu);
-        acc += x * q;
-    }
-    return acc;
+    for (int j = 0; j < 4; ++j) acc = __dp4a(w[j], codes4(t, 4 * j, tbl), acc);
+    return static_cast<int>(acc);
 }
 
 // Two consecutive steps of uint8 codes (elements at ip and ip + stride,
@@ -199,24 +208,18 @@ __device__ __forceinline__ int partial2(const uint16_t* ip, const uint8_t* vp, i
         ldg256(ip + stride, t2);
         v2 = __ldg(reinterpret_cast<const uint4*>(vp + stride));
     }
-    int acc = 0;
+    uint32_t acc = 0;
     {
         const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-        for (int u = 0; u < 16; ++u) {
-            const int q = static_cast<int>(tbl[term_of(t, u)]);
-            acc += static_cast<int>((w[u >> 2] >> (8 * (u & 3))) & 0xffu) * q;
-        }
+        for (int j = 0; j < 4; ++j) acc = __dp4a(w[j], codes4(t, 4 * j, tbl), acc);
     }
     if (rem2 > 0) {
         const uint32_t w[4] = {v2.x, v2.y, v2.z, v2.w};
 #pragma unroll
-        for (int u = 0; u < 16; ++u) {
-            const int q = static_cast<int>(tbl[term_of(t2, u)]);
-            acc += static_cast<int>((w[u >> 2] >> (8 * (u & 3))) & 0xffu) * q;
-        }
+        for (int j = 0; j < 4; ++j) acc = __dp4a(w[j], codes4(t2, 4 * j, tbl), acc);
     }
-    return acc;
+    return static_cast<int>(acc);
 }
 
 // uint16 codes: int64 sum (distance.h:49-57).
@@ -473,7 +476,7 @@ __device__ int gather(const SeismicLaunch& a, Cursor& c, bool first, int64_t lb0
             g.blk = c.split_blk;
             g.bs = c.split_bs;
             g.head = 0;
-            g.pad = 0;
+            g.surv = 0;
             segs[0] = g;
         }
         nseg = 1;
@@ -532,7 +535,7 @@ __device__ int gather(const SeismicLaunch& a, Cursor& c, bool first, int64_t lb0
             g.blk = blk;
             g.bs = bs;
             g.head = 1;
-            g.pad = 0;
+            g.surv = 0;
             segs[nseg + r] = g;
         }
         int taken_docs = 0;
@@ -759,8 +762,11 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
 
         int n = 0;  // heap size (warp 0)
         bool first = true;
+        // docs_scored / row_bytes: every thread adds the member docs of each
+        // batch it checks after scoring; warp 0 takes back those of segments
+        // the second test drops (two's-complement sums, exact in the total)
         unsigned long long docs_scored = 0, blocks_visited = 0, bytes = 0, lists = 0,
-                           lane_bytes = 0;
+                           row_bytes = 0;
         for (int c = 0; c < ncut; ++c) {
             // 3. summary scores of the next nwarps lists, one warp per list
             if (c % nwarps == 0) {
@@ -815,6 +821,7 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                             ctl->nseg = nseg;
                             ctl->total = total;
                             ctl->next = 0;
+                            ctl->nheap = n;
                         }
                     }
                     __syncthreads();
@@ -862,120 +869,128 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                         if constexpr (kCl) cluster_sync();
                         __syncthreads();
                     }
-                    // 7. second pruning test and heap offers, in block order
+                    // 7. second pruning test and heap offers, in block order.
+                    // (a) All threads: a doc can still enter the heap only if
+                    // it is a member scoring above the heap minimum as it
+                    // stood when the batch was gathered (the minimum only
+                    // grows); such docs are counted per segment.
+                    {
+                        const int nh = ctl->nheap;
+                        const float hmin0 = nh == a.k ? hs[a.k - 1] : 0.0f;
+                        for (int i = tid; i < total; i += blockDim.x) {
+                            if (cdoc[i] >= 0) {
+                                ++docs_scored;
+                                row_bytes += 8ull + static_cast<unsigned long long>(clen[i]) *
+                                                        (2 + vsz);
+                                if (nh < a.k || csc[i] > hmin0) atomicAdd(&segs[cseg[i]].surv, 1);
+                            }
+                        }
+                        __syncthreads();
+                    }
+                    // (b) Warp 0 walks the segments in block order as the
+                    // reference walks its blocks (seismic_index.cpp:78-117):
+                    // each block head is tested against the heap as it stands
+                    // at its turn, then its docs are offered in order. A run
+                    // of segments without survivors leaves the heap as it is,
+                    // so all its tests see one minimum and one ballot settles
+                    // up to 32 of them; a segment with survivors offers those.
                     if (warp == 0) {
-                        // One segment exactly as the reference walks it: the
-                        // block's test against the heap as it stands, then
-                        // its docs offered in order. True when the first
-                        // list's walk ends here.
-                        auto walk_segment = [&](int s) -> bool {
-                            const Seg g = segs[s];
-                            if (g.head) {
-                                if (n == a.k && __fmul_rn(g.bs, a.heap_factor) < hs[a.k - 1]) {
-                                    if (first) {
-                                        cur.dead = true;
-                                        cur.split = false;
-                                        return true;
-                                    }
-                                    if (s == nseg - 1) cur.split = false;
-                                    return false;
-                                }
-                                ++blocks_visited;
-                                bytes += 16;
-                            }
-                            bytes += 4ull * static_cast<unsigned long long>(g.cnt);
-                            for (int b = 0; b < g.cnt; b += 32) {
-                                const int j = b + lane;
-                                float sc = 0.0f;
-                                int32_t d = -1;
-                                if (j < g.cnt) {
-                                    d = cdoc[g.cand0 + j];
-                                    sc = csc[g.cand0 + j];
-                                }
-                                const bool mem = d >= 0;
-                                if (mem)
-                                    lane_bytes += 8ull + static_cast<unsigned long long>(
-                                                             clen[g.cand0 + j]) * (2 + vsz);
-                                docs_scored += __popc(__ballot_sync(kFull, mem));
-                                unsigned m =
-                                    __ballot_sync(kFull, mem && (n < a.k || sc > hs[a.k - 1]));
-                                while (m) {
-                                    const int src = __ffs(m) - 1;
-                                    m &= m - 1;
-                                    const float S = __shfl_sync(kFull, sc, src);
-                                    const int32_t D = __shfl_sync(kFull, d, src);
-                                    heap_offer(S, D, hs, hid, n, a.k, lane);
+                        // the work counters give back a dropped segment's docs
+                        auto give_back = [&](int t) {
+                            const Seg g = segs[t];
+                            for (int j = lane; j < g.cnt; j += 32) {
+                                const int i = g.cand0 + j;
+                                if (cdoc[i] >= 0) {
+                                    --docs_scored;
+                                    row_bytes -= 8ull + static_cast<unsigned long long>(clen[i]) *
+                                                            (2 + vsz);
                                 }
                             }
-                            return false;
                         };
-                        // Windows of whole segments with at most 32 docs in
-                        // all, one doc per lane. While the heap is full and no
-                        // doc of a window beats its minimum, walking the
-                        // window changes nothing in the heap, so every block
-                        // test in it sees the same minimum: one pass settles
-                        // the window. Otherwise (or for a larger segment) the
-                        // window is walked segment by segment.
+                        auto end_first_list = [&](int from) {
+                            for (int t = from; t < nseg; ++t) give_back(t);
+                            cur.dead = true;
+                            cur.split = false;
+                        };
                         int s = 0;
-                        while (s < nseg) {
-                            const int base = segs[s].cand0;
+                        bool ended = false;
+                        while (s < nseg && !ended) {
                             const int sl = s + lane;
                             const bool valid = sl < nseg;
-                            int end = INT_MAX, head = 0, cnt = 0;
+                            int head = 0, cnt = 0, surv = 0;
                             float bs = 0.0f;
                             if (valid) {
                                 const Seg g = segs[sl];
-                                end = g.cand0 + g.cnt - base;
                                 head = g.head;
                                 cnt = g.cnt;
+                                surv = g.surv;
                                 bs = g.bs;
                             }
-                            // segment ends grow with the index: a prefix fits
-                            const int w = __popc(__ballot_sync(kFull, valid && end <= 32));
-                            bool stop = false;
-                            if (w == 0 || n < a.k) {
-                                const int e = w == 0 ? s + 1 : s + w;
-                                for (int t = s; t < e && !stop; ++t) stop = walk_segment(t);
-                                if (stop) break;
-                                s = e;
-                                continue;
-                            }
-                            const float hmin = hs[a.k - 1];
+                            const int w = __popc(__ballot_sync(kFull, valid));
+                            const unsigned sm = __ballot_sync(kFull, valid && surv > 0);
+                            const int S = sm ? __ffs(sm) - 1 : w;  // first that may change the heap
+                            const bool full = n == a.k;
+                            const float hmin = full ? hs[a.k - 1] : 0.0f;
                             const bool fail =
-                                lane < w && head && __fmul_rn(bs, a.heap_factor) < hmin;
-                            const unsigned failm = __ballot_sync(kFull, fail);
+                                lane < S && head && full && __fmul_rn(bs, a.heap_factor) < hmin;
+                            const unsigned fm = __ballot_sync(kFull, fail);
                             // the first list ends at its first failing block
-                            const int wl = (first && failm) ? __ffs(failm) - 1 : w;
-                            const int ndocs = wl > 0 ? __shfl_sync(kFull, end, wl - 1) : 0;
-                            bool mem = false;
-                            float sc = 0.0f;
-                            if (lane < ndocs) {
-                                const int rs = static_cast<int>(cseg[base + lane]) - s;
-                                mem = !((failm >> rs) & 1u) && cdoc[base + lane] >= 0;
-                                sc = csc[base + lane];
+                            const int upto = (first && fm) ? __ffs(fm) - 1 : S;
+                            const bool taken = lane < upto && !fail;
+                            blocks_visited += __popc(__ballot_sync(kFull, taken && head));
+                            bytes += 16ull * __popc(__ballot_sync(kFull, taken && head)) +
+                                     4ull * __reduce_add_sync(kFull, taken ? cnt : 0);
+                            unsigned dm = __ballot_sync(kFull, lane < upto && fail);
+                            while (dm) {  // later lists skip a failing block
+                                const int t = __ffs(dm) - 1;
+                                dm &= dm - 1;
+                                give_back(s + t);
+                                if (s + t == nseg - 1) cur.split = false;
                             }
-                            if (__any_sync(kFull, mem && sc > hmin)) {
-                                for (int t = s; t < s + w && !stop; ++t) stop = walk_segment(t);
-                                if (stop) break;
-                                s += w;
-                                continue;
-                            }
-                            const bool took = lane < wl && !fail;
-                            const unsigned heads = __ballot_sync(kFull, took && head);
-                            blocks_visited += __popc(heads);
-                            bytes += 16ull * __popc(heads) +
-                                     4ull * __reduce_add_sync(kFull, took ? cnt : 0);
-                            if (mem)
-                                lane_bytes += 8ull + static_cast<unsigned long long>(
-                                                         clen[base + lane]) * (2 + vsz);
-                            docs_scored += __popc(__ballot_sync(kFull, mem));
-                            if (wl < w) {
-                                cur.dead = true;
-                                cur.split = false;
+                            if (first && fm) {
+                                end_first_list(s + upto);
+                                ended = true;
                                 break;
                             }
-                            if (s + w == nseg && ((failm >> (w - 1)) & 1u)) cur.split = false;
-                            s += w;
+                            s += upto;
+                            if (upto == w) continue;
+                            // segment s holds survivors: its test, then its offers
+                            const Seg g = segs[s];
+                            if (g.head && n == a.k &&
+                                __fmul_rn(g.bs, a.heap_factor) < hs[a.k - 1]) {
+                                if (first) {
+                                    end_first_list(s);
+                                    ended = true;
+                                    break;
+                                }
+                                give_back(s);
+                                if (s == nseg - 1) cur.split = false;
+                            } else {
+                                if (g.head) {
+                                    ++blocks_visited;
+                                    bytes += 16;
+                                }
+                                bytes += 4ull * static_cast<unsigned long long>(g.cnt);
+                                for (int b = 0; b < g.cnt; b += 32) {
+                                    const int j = b + lane;
+                                    float sc = 0.0f;
+                                    int32_t d = -1;
+                                    if (j < g.cnt) {
+                                        d = cdoc[g.cand0 + j];
+                                        sc = csc[g.cand0 + j];
+                                    }
+                                    unsigned m = __ballot_sync(
+                                        kFull, d >= 0 && (n < a.k || sc > hs[a.k - 1]));
+                                    while (m) {
+                                        const int src = __ffs(m) - 1;
+                                        m &= m - 1;
+                                        const float S2 = __shfl_sync(kFull, sc, src);
+                                        const int32_t D2 = __shfl_sync(kFull, d, src);
+                                        heap_offer(S2, D2, hs, hid, n, a.k, lane);
+                                    }
+                                }
+                            }
+                            ++s;
                         }
                     }
                 }
@@ -1003,18 +1018,24 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                     ol[i] = -1;
                 }
             }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) lane_bytes += __shfl_xor_sync(kFull, lane_bytes, o);
         }
-        // lane 0 of every warp adds the warp's summary bytes
-        if (a.stats != nullptr && lane == 0) {
-            if (warp == 0) {
-                atomicAdd(a.stats + kStatDocsScored, docs_scored);
-                atomicAdd(a.stats + kStatBlocksVisited, blocks_visited);
-                atomicAdd(a.stats + kStatListsProbed, lists);
-                bytes += lane_bytes;
+        if (a.stats != nullptr) {
+            // per warp: its threads' doc counts and row bytes, plus its
+            // summary bytes (the same on every lane) and, for warp 0, the
+            // block counts
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                row_bytes += __shfl_xor_sync(kFull, row_bytes, o);
+                docs_scored += __shfl_xor_sync(kFull, docs_scored, o);
             }
-            atomicAdd(a.stats + kStatBytes, bytes);
+            if (lane == 0) {
+                if (warp == 0) {
+                    atomicAdd(a.stats + kStatBlocksVisited, blocks_visited);
+                    atomicAdd(a.stats + kStatListsProbed, lists);
+                }
+                atomicAdd(a.stats + kStatDocsScored, docs_scored);
+                atomicAdd(a.stats + kStatBytes, bytes + row_bytes);
+            }
         }
         // restore the all-zero table for the next query
         __syncthreads();

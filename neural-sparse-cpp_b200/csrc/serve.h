@@ -96,7 +96,7 @@ private:
     Index* index_;
     ServerConfig cfg_;
     SeismicState* st_ = nullptr;
-    const std::vector<idx_t>* id_map_ = nullptr;
+    const std::vector<int64_t>* id_map_ = nullptr;
     int dim_ = 0;
     int device_ = 0;
     std::vector<int64_t> ext_ids_;

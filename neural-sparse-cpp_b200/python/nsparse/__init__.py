@@ -50,6 +50,9 @@ _sig("nsp_index_factory", ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(_P))
 _sig("nsp_index_free", _P)
 _sig("nsp_index_add", _P, _I32, _P, _P, _P)
 _sig("nsp_index_add_with_ids", _P, _I32, _P, _P, _P, _P)
+_sig("nsp_index_add_with_ids64", _P, _I32, _P, _P, _P, _P)
+_sig("nsp_index_search64", _P, _I32, _P, _P, _P, ctypes.c_int, _P, _P, _P)
+_sig("nsp_id_selector_set64_new", ctypes.c_size_t, _P, ctypes.POINTER(_P))
 _sig("nsp_index_build", _P)
 _sig("nsp_index_search", _P, _I32, _P, _P, _P, ctypes.c_int, _P, _P, _P)
 _sig("nsp_index_num_vectors", _P, ctypes.POINTER(ctypes.c_int64))
@@ -180,6 +183,17 @@ class SetIDSelector(IDSelector):
         self._h = h.value
 
 
+class SetIDSelector64(IDSelector):
+    """Extension: a set of 64-bit ids, for an IDMapIndex whose external ids
+    need them."""
+
+    def __init__(self, ids):
+        ids = _typed(ids, np.int64, "indices")
+        h = _P()
+        _check(_L.nsp_id_selector_set64_new(len(ids), _ptr(ids), ctypes.byref(h)))
+        self._h = h.value
+
+
 class ArrayIDSelector(IDSelector):
     def __init__(self, ids):
         ids = _typed(ids, np.int32, "indices")
@@ -298,6 +312,30 @@ class Index:
         ids = np.ascontiguousarray(ids, dtype=np.int32)
         _check(_L.nsp_index_add_with_ids(self._h, int(n), _ptr(indptr), _ptr(indices),
                                          _ptr(values), _ptr(ids)))
+
+    def add_with_ids64(self, n, indptr, indices, values, ids):
+        """Extension: add_with_ids with 64-bit external ids (IDMapIndex)."""
+        indptr = _typed(indptr, np.int32, "indptr")
+        indices = _typed(indices, np.uint16, "indices")
+        values = _typed(values, np.float32, "values")
+        ids = _typed(ids, np.int64, "ids")
+        _check(_L.nsp_index_add_with_ids64(self._h, int(n), _ptr(indptr), _ptr(indices),
+                                           _ptr(values), _ptr(ids)))
+
+    def search64(self, n, indptr, indices, values, k, params=None):
+        """Extension: search with int64 labels (an IDMapIndex's 64-bit ids)."""
+        indptr = np.ascontiguousarray(indptr, dtype=np.int32)
+        indices = np.ascontiguousarray(indices, dtype=np.uint16)
+        values = np.ascontiguousarray(values, dtype=np.float32)
+        n, k = int(n), int(k)
+        if n <= 0 or k <= 0:
+            raise ValueError("value must be positive")
+        distances = np.empty((n, k), dtype=np.float32)
+        labels = np.empty((n, k), dtype=np.int64)
+        _check(_L.nsp_index_search64(self._h, n, _ptr(indptr), _ptr(indices), _ptr(values), k,
+                                     _ptr(distances), _ptr(labels),
+                                     None if params is None else params._h))
+        return distances, labels
 
     def build(self):
         _check(_L.nsp_index_build(self._h))
