@@ -85,7 +85,7 @@ struct Ctl {
 __host__ __device__ inline size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
 
 struct CtaLayout {
-    size_t tbl, qv, qterm, qraw, cuts, hs, hid, cdoc, coff, clen, csc, segs, cseg, total;
+    size_t tbl, qv, qterm, qraw, cuts, hs, hid, cdoc, coff, clen, csc, segs, cseg, wsum, total;
 };
 
 // Shared-memory layout of one CTA. The four candidate arrays are contiguous
@@ -107,6 +107,7 @@ __host__ __device__ inline CtaLayout cta_layout(int vsize, int tsize, int dim, i
     L.csc = o;   o += static_cast<size_t>(batch) * 4;
     L.segs = o;  o += static_cast<size_t>(seg_cap) * sizeof(Seg);
     L.cseg = o;  o += a16(static_cast<size_t>(batch) * 2);
+    L.wsum = o;  o += 32 * 4;
     L.total = o;
     return L;
 }
@@ -165,20 +166,9 @@ __device__ __forceinline__ void products(const uint16_t* ip, const float* vp, in
     }
 }
 
-// The query codes of row terms u0..u0+3, packed one byte each (byte j = the
-// code of term u0+j) so that one __dp4a multiplies them with the four doc
-// codes a values word holds and adds the four products.
-template <typename TE>
-__device__ __forceinline__ uint32_t codes4(const uint32_t (&t)[8], int u0, const TE* tbl) {
-    const uint32_t q0 = tbl[term_of(t, u0)];
-    const uint32_t q1 = tbl[term_of(t, u0 + 1)];
-    const uint32_t q2 = tbl[term_of(t, u0 + 2)];
-    const uint32_t q3 = tbl[term_of(t, u0 + 3)];
-    return __byte_perm(__byte_perm(q0, q1, 0x3240), __byte_perm(q2, q3, 0x3240), 0x5410);
-}
-
 // uint8 codes: the sum of code products as int (distance.h:39-47); padding
-// codes are 0. Sums of at most 2^16 products of two codes stay below 2^32.
+// codes are 0. (Packing four looked-up codes for __dp4a measured slower: the
+// packing waits for all four lookups.)
 template <typename TE>
 __device__ __forceinline__ int partial(const uint16_t* ip, const uint8_t* vp, int rem,
                                        const TE* tbl) {
@@ -187,10 +177,14 @@ __device__ __forceinline__ int partial(const uint16_t* ip, const uint8_t* vp, in
     ldg256(ip, t);
     const uint4 v = __ldg(reinterpret_cast<const uint4*>(vp));
     const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-    uint32_t acc = 0;
+    int acc = 0;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc = __dp4a(w[j], codes4(t, 4 * j, tbl), acc);
-    return static_cast<int>(acc);
+    for (int u = 0; u < 16; ++u) {
+        const int q = static_cast<int>(tbl[term_of(t, u)]);
+        const int x = static_cast<int>((w[u >> 2] >> (8 * (u & 3))) & 0xffu);
+        acc += x * q;
+    }
+    return acc;
 }
 
 // Two consecutive steps of uint8 codes (elements at ip and ip + stride,
@@ -208,18 +202,24 @@ __device__ __forceinline__ int partial2(const uint16_t* ip, const uint8_t* vp, i
         ldg256(ip + stride, t2);
         v2 = __ldg(reinterpret_cast<const uint4*>(vp + stride));
     }
-    uint32_t acc = 0;
+    int acc = 0;
     {
         const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc = __dp4a(w[j], codes4(t, 4 * j, tbl), acc);
+        for (int u = 0; u < 16; ++u) {
+            const int q = static_cast<int>(tbl[term_of(t, u)]);
+            acc += static_cast<int>((w[u >> 2] >> (8 * (u & 3))) & 0xffu) * q;
+        }
     }
     if (rem2 > 0) {
         const uint32_t w[4] = {v2.x, v2.y, v2.z, v2.w};
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc = __dp4a(w[j], codes4(t2, 4 * j, tbl), acc);
+        for (int u = 0; u < 16; ++u) {
+            const int q = static_cast<int>(tbl[term_of(t2, u)]);
+            acc += static_cast<int>((w[u >> 2] >> (8 * (u & 3))) & 0xffu) * q;
+        }
     }
-    return static_cast<int>(acc);
+    return acc;
 }
 
 // uint16 codes: int64 sum (distance.h:49-57).
@@ -351,7 +351,7 @@ __device__ void score_batch(const FwdView& fwd, Ctl* ctl, const TE* tbl, const f
 template <typename V>
 __device__ void list_summaries(const SeismicLaunch& a, int t, int nb, const uint16_t* qterm,
                                const V* qraw, int qn, float* bscore, int lane,
-                               unsigned long long& bytes) {
+                               uint32_t& bytes) {
     constexpr int vsz = static_cast<int>(sizeof(V));
     // uint8 codes: a block's score is a sum of at most qn products of two
     // codes (<= 255 * 255 each), an integer below 2^24 -- exact in fp32 --
@@ -380,16 +380,16 @@ __device__ void list_summaries(const SeismicLaunch& a, int t, int nb, const uint
                 hit = true;
             }
         }
-        bytes += 8ull * static_cast<unsigned long long>(min(32, qn - i0));
+        bytes += 8u * static_cast<uint32_t>(min(32, qn - i0));
         unsigned hm = __ballot_sync(kFull, hit);
-        bytes += 16ull * __popc(hm);
+        bytes += 16u * __popc(hm);
         while (hm) {
             const int src = __ffs(hm) - 1;
             hm &= hm - 1;
             const int64_t R0 = __shfl_sync(kFull, r0, src);
             const int64_t R1 = __shfl_sync(kFull, r1, src);
             const float QV = __shfl_sync(kFull, qv, src);
-            bytes += static_cast<unsigned long long>(R1 - R0) * (2 + vsz);
+            bytes += static_cast<uint32_t>(R1 - R0) * (2 + vsz);
             const V* sv = static_cast<const V*>(a.ix.sval);
             if (exact_any_order) {
                 // integer products and sums below 2^24: every order of the
@@ -458,8 +458,10 @@ struct Cursor {
 };
 
 // Warp 0: fills the next batch with segments of blocks that pass the pruning
-// test against the current heap. Returns the number of segments; `total`
-// receives the number of docs.
+// test against the current heap, taking blocks in the list's visiting order
+// `order[0..nb)` (the first list: sorted; later lists: the blocks that passed
+// when the list began, in block order). Returns the number of segments;
+// `total` receives the number of docs.
 __device__ int gather(const SeismicLaunch& a, Cursor& c, bool first, int64_t lb0, int nb,
                       const float* bscore, const uint16_t* order, int n, const float* hs,
                       Seg* segs, int batch, int seg_cap, int& total, int lane) {
@@ -493,9 +495,13 @@ __device__ int gather(const SeismicLaunch& a, Cursor& c, bool first, int64_t lb0
         const bool in = p < nb;
         int blk = 0;
         float bs = 0.0f;
+        int64_t d0 = 0, d1 = 0;
         if (in) {
-            blk = first ? static_cast<int>(order[p]) : p;
+            blk = static_cast<int>(order[p]);
+            // the block's doc range is loaded with its score, before the test
             bs = __ldcg(bscore + blk);
+            d0 = __ldg(a.ix.bdp + lb0 + blk);
+            d1 = __ldg(a.ix.bdp + lb0 + blk + 1);
         }
         const bool pass = in && !(full && __fmul_rn(bs, a.heap_factor) < hmin);
         const unsigned inm = __ballot_sync(kFull, in);
@@ -510,12 +516,7 @@ __device__ int gather(const SeismicLaunch& a, Cursor& c, bool first, int64_t lb0
             }
         }
         const bool cand = pass && lane < lim;
-        int64_t d0 = 0;
-        int sz = 0;
-        if (cand) {
-            d0 = __ldg(a.ix.bdp + lb0 + blk);
-            sz = static_cast<int>(__ldg(a.ix.bdp + lb0 + blk + 1) - d0);
-        }
+        const int sz = cand ? static_cast<int>(d1 - d0) : 0;
         int incl = sz;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -573,6 +574,34 @@ __device__ int gather(const SeismicLaunch& a, Cursor& c, bool first, int64_t lb0
     return nseg;
 }
 
+// All threads: the blocks of a later list that pass the pruning test against
+// the heap as it stands when the list begins, in block order, into
+// order[0..return). The heap minimum only grows, so a block failing now fails
+// at its turn too; the walk then visits only these (the reference tests and
+// skips every block, seismic_index.cpp:78-86).
+__device__ int passing_blocks(const float* bscore, int nb, bool full, float hmin, float hf,
+                              uint16_t* order, int* wsum, int tid, int lane, int warp,
+                              int nwarps) {
+    int base = 0;
+    for (int i0 = 0; i0 < nb; i0 += nwarps * 32) {
+        const int i = i0 + tid;
+        const bool pass = i < nb && !(full && __fmul_rn(__ldcg(bscore + i), hf) < hmin);
+        const unsigned m = __ballot_sync(kFull, pass);
+        if (lane == 0) wsum[warp] = __popc(m);
+        __syncthreads();
+        int off = 0, all = 0;
+        for (int w = 0; w < nwarps; ++w) {
+            const int c = wsum[w];
+            off += w < warp ? c : 0;
+            all += c;
+        }
+        if (pass) order[base + off + __popc(m & ((1u << lane) - 1u))] = static_cast<uint16_t>(i);
+        base += all;
+        __syncthreads();
+    }
+    return base;
+}
+
 // A cluster's CTAs meet here (barrier.cluster arrive + wait: release and
 // acquire of shared memory across the cluster).
 __device__ __forceinline__ void cluster_sync() { cg::this_cluster().sync(); }
@@ -610,6 +639,7 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
     float* csc = reinterpret_cast<float*>(smem + L.csc);
     Seg* segs = reinterpret_cast<Seg*>(smem + L.segs);
     uint16_t* cseg = reinterpret_cast<uint16_t*>(smem + L.cseg);  // each candidate's segment
+    int* wsum = reinterpret_cast<int*>(smem + L.wsum);
 
     const int maxb = a.ix.max_blocks;
     float* bscore_cta = a.bscore + static_cast<size_t>(blockIdx.x) * nwarps * maxb;
@@ -703,6 +733,7 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
             else
                 q = a.first_query + static_cast<int>(cid) + iter * static_cast<int>(ncl);
             ctl->q = q;
+            ctl->nheap = 0;  // the query's heap starts empty
             if constexpr (kCl) push_to_cluster(&ctl->q, q);
         }
         ++iter;
@@ -762,11 +793,12 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
 
         int n = 0;  // heap size (warp 0)
         bool first = true;
+        // Counters of this query (32 bits: a query reads far less than 4 GB).
         // docs_scored / row_bytes: every thread adds the member docs of each
         // batch it checks after scoring; warp 0 takes back those of segments
-        // the second test drops (two's-complement sums, exact in the total)
-        unsigned long long docs_scored = 0, blocks_visited = 0, bytes = 0, lists = 0,
-                           row_bytes = 0;
+        // the second test drops, so a thread's value may be negative.
+        uint32_t blocks_visited = 0, bytes = 0, lists = 0;
+        int32_t docs_scored = 0, row_bytes = 0;
         for (int c = 0; c < ncut; ++c) {
             // 3. summary scores of the next nwarps lists, one warp per list
             if (c % nwarps == 0) {
@@ -790,7 +822,9 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
             if (nb > 0) {
                 ++lists;
                 const float* bscore = bscore_cta + static_cast<size_t>(c % nwarps) * maxb;
-                // 4. visiting order of the first list
+                // 4. visiting order: the first list's blocks sorted; a later
+                // list's blocks that can still pass, in block order
+                int nbv = nb;
                 if (first) {
                     int p2 = 1;
                     while (p2 < nb) p2 <<= 1;
@@ -802,6 +836,10 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                         break;
                     }
                     sort_blocks(bscore, nb, keys, p2, order, tid, blockDim.x);
+                } else {
+                    const int nh = ctl->nheap;
+                    nbv = passing_blocks(bscore, nb, nh == a.k, nh == a.k ? hs[a.k - 1] : 0.0f,
+                                         a.heap_factor, order, wsum, tid, lane, warp, nwarps);
                 }
                 // 5. batches
                 Cursor cur;
@@ -815,7 +853,7 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                 for (;;) {
                     if (warp == 0) {
                         int total = 0;
-                        const int nseg = gather(a, cur, first, lb0, nb, bscore, order, n, hs,
+                        const int nseg = gather(a, cur, first, lb0, nbv, bscore, order, n, hs,
                                                 segs, batch, a.seg_cap, total, lane);
                         if (lane == 0) {
                             ctl->nseg = nseg;
@@ -880,8 +918,7 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                         for (int i = tid; i < total; i += blockDim.x) {
                             if (cdoc[i] >= 0) {
                                 ++docs_scored;
-                                row_bytes += 8ull + static_cast<unsigned long long>(clen[i]) *
-                                                        (2 + vsz);
+                                row_bytes += 8 + static_cast<int32_t>(clen[i]) * (2 + vsz);
                                 if (nh < a.k || csc[i] > hmin0) atomicAdd(&segs[cseg[i]].surv, 1);
                             }
                         }
@@ -902,8 +939,7 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                                 const int i = g.cand0 + j;
                                 if (cdoc[i] >= 0) {
                                     --docs_scored;
-                                    row_bytes -= 8ull + static_cast<unsigned long long>(clen[i]) *
-                                                            (2 + vsz);
+                                    row_bytes -= 8 + static_cast<int32_t>(clen[i]) * (2 + vsz);
                                 }
                             }
                         };
@@ -938,8 +974,8 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                             const int upto = (first && fm) ? __ffs(fm) - 1 : S;
                             const bool taken = lane < upto && !fail;
                             blocks_visited += __popc(__ballot_sync(kFull, taken && head));
-                            bytes += 16ull * __popc(__ballot_sync(kFull, taken && head)) +
-                                     4ull * __reduce_add_sync(kFull, taken ? cnt : 0);
+                            bytes += 16u * __popc(__ballot_sync(kFull, taken && head)) +
+                                     4u * __reduce_add_sync(kFull, taken ? cnt : 0);
                             unsigned dm = __ballot_sync(kFull, lane < upto && fail);
                             while (dm) {  // later lists skip a failing block
                                 const int t = __ffs(dm) - 1;
@@ -970,7 +1006,7 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                                     ++blocks_visited;
                                     bytes += 16;
                                 }
-                                bytes += 4ull * static_cast<unsigned long long>(g.cnt);
+                                bytes += 4u * static_cast<uint32_t>(g.cnt);
                                 for (int b = 0; b < g.cnt; b += 32) {
                                     const int j = b + lane;
                                     float sc = 0.0f;
@@ -1030,11 +1066,17 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
             }
             if (lane == 0) {
                 if (warp == 0) {
-                    atomicAdd(a.stats + kStatBlocksVisited, blocks_visited);
-                    atomicAdd(a.stats + kStatListsProbed, lists);
+                    atomicAdd(a.stats + kStatBlocksVisited,
+                              static_cast<unsigned long long>(blocks_visited));
+                    atomicAdd(a.stats + kStatListsProbed, static_cast<unsigned long long>(lists));
                 }
-                atomicAdd(a.stats + kStatDocsScored, docs_scored);
-                atomicAdd(a.stats + kStatBytes, bytes + row_bytes);
+                // a warp's net counts can be negative: widened with their sign,
+                // they add up modulo 2^64 to the exact total
+                atomicAdd(a.stats + kStatDocsScored,
+                          static_cast<unsigned long long>(static_cast<long long>(docs_scored)));
+                atomicAdd(a.stats + kStatBytes,
+                          static_cast<unsigned long long>(bytes) +
+                              static_cast<unsigned long long>(static_cast<long long>(row_bytes)));
             }
         }
         // restore the all-zero table for the next query
