@@ -70,7 +70,7 @@ struct Seg {
     int32_t blk;    // block index within its list
     float bs;       // the block's summary score
     int32_t head;   // 1 when the block starts here (its pruning test applies)
-    int32_t surv;   // docs that may still enter the heap (counted after scoring)
+    int32_t surv;   // 1 when a doc of it may still enter the heap (set after scoring)
 };
 
 struct Ctl {
@@ -911,7 +911,7 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                     // (a) All threads: a doc can still enter the heap only if
                     // it is a member scoring above the heap minimum as it
                     // stood when the batch was gathered (the minimum only
-                    // grows); such docs are counted per segment.
+                    // grows); segments holding such docs are flagged.
                     {
                         const int nh = ctl->nheap;
                         const float hmin0 = nh == a.k ? hs[a.k - 1] : 0.0f;
@@ -919,7 +919,8 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                             if (cdoc[i] >= 0) {
                                 ++docs_scored;
                                 row_bytes += 8 + static_cast<int32_t>(clen[i]) * (2 + vsz);
-                                if (nh < a.k || csc[i] > hmin0) atomicAdd(&segs[cseg[i]].surv, 1);
+                                // a flag: every writer stores the same 1
+                                if (nh < a.k || csc[i] > hmin0) segs[cseg[i]].surv = 1;
                             }
                         }
                         __syncthreads();

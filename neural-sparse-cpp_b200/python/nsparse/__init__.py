@@ -171,7 +171,7 @@ class IDSelector:
 
     def __del__(self):
         h, self._h = self._h, None
-        if h:
+        if h and _L is not None:  # at interpreter exit the module may be gone
             _L.nsp_id_selector_free(h)
 
 
@@ -259,7 +259,7 @@ class SearchParameters:
 
     def __del__(self):
         h, self._h = getattr(self, "_h", None), None
-        if h:
+        if h and _L is not None:  # at interpreter exit the module may be gone
             _L.nsp_search_params_free(h)
 
 
@@ -398,7 +398,7 @@ class Index:
 
     def __del__(self):
         h, self._h = getattr(self, "_h", None), None
-        if h:
+        if h and _L is not None:  # at interpreter exit the module may be gone
             _L.nsp_index_free(h)
 
 
