@@ -32,6 +32,11 @@ struct EngineOptions {
     // 2, 4 or 8 a thread-block cluster whose CTAs score each query's batches
     // together (lower latency per query; identical results).
     int ctas_per_query = 0;
+    // Batched SEISMIC search on variants 2-5 only: a slower counting pass
+    // that also counts each scored doc's row once per query, as the
+    // reference's visited set does (SearchStats::unique_*); results are the
+    // same.
+    bool count_unique = false;
 };
 
 struct SearchParameters {
@@ -48,10 +53,17 @@ private:
 struct SearchStats {
     uint64_t docs_scored = 0;
     uint64_t blocks_visited = 0;
-    uint64_t bytes = 0;          // algorithmic bytes the kernels read
+    uint64_t bytes = 0;          // bytes the kernels read, rows as often as scored
     uint64_t lists_probed = 0;
     float kernel_ms = 0.0f;
     int launches = 0;
+    uint64_t row_bytes = 0;      // the rows' share of `bytes`
+    // Counting pass (EngineOptions::count_unique) only: docs and row bytes
+    // counted once per query. The reference's algorithmic bytes are then
+    // bytes - row_bytes + unique_row_bytes (SEISMIC scores a doc met again in
+    // a later list again; the reference skips it).
+    uint64_t unique_docs = 0;
+    uint64_t unique_row_bytes = 0;
 };
 const SearchStats& last_search_stats();
 

@@ -160,6 +160,11 @@ nsp_status_t nsp_search_params_set_kernel(nsp_search_params_t* params, int varia
  * candidates together, for lower latency per query). Results do not depend on
  * it. */
 nsp_status_t nsp_search_params_set_split(nsp_search_params_t* params, int ctas_per_query);
+/* Extension: count_unique != 0 makes a batched SEISMIC search (kernel variants
+ * 2-5) a counting pass: slower, same results, and its stats also count each
+ * scored doc's row once per query, as the reference's visited set does
+ * (nsp_search_stats_t.unique_*). */
+nsp_status_t nsp_search_params_set_count_unique(nsp_search_params_t* params, int count_unique);
 nsp_status_t nsp_search_params_free(nsp_search_params_t* params);
 
 /* ---- engine extensions -------------------------------------------------- */
@@ -171,6 +176,9 @@ typedef struct {
     uint64_t lists_probed;
     float kernel_ms;       /* device time of the search kernels */
     int32_t launches;
+    uint64_t row_bytes;    /* the rows' share of `bytes` (rows as often as scored) */
+    uint64_t unique_docs;  /* counting pass only: docs counted once per query */
+    uint64_t unique_row_bytes;  /* counting pass only: their rows' bytes */
 } nsp_search_stats_t;
 
 /* Counters of the calling thread's last nsp_index_search. */

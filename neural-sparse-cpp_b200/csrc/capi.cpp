@@ -321,6 +321,13 @@ nsp_status_t nsp_search_params_set_split(nsp_search_params_t* params, int ctas_p
     });
 }
 
+nsp_status_t nsp_search_params_set_count_unique(nsp_search_params_t* params, int count_unique) {
+    return guarded([&] {
+        if (params == nullptr) throw std::invalid_argument("unexpected nullptr");
+        as_params(params)->engine.count_unique = count_unique != 0;
+    });
+}
+
 nsp_status_t nsp_search_params_free(nsp_search_params_t* params) {
     return guarded([&] { delete as_params(params); });
 }
@@ -335,6 +342,9 @@ nsp_status_t nsp_last_search_stats(nsp_search_stats_t* out) {
         out->lists_probed = s.lists_probed;
         out->kernel_ms = s.kernel_ms;
         out->launches = s.launches;
+        out->row_bytes = s.row_bytes;
+        out->unique_docs = s.unique_docs;
+        out->unique_row_bytes = s.unique_row_bytes;
     });
 }
 

@@ -677,8 +677,24 @@ void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
     auto* err = static_cast<int32_t*>(ws.dev(Workspace::kErr, sizeof(int32_t)));
     cuda_check(cudaMemsetAsync(err, 0, sizeof(int32_t), s), "memset");
     a.err = err;
+    if (args.count_unique && (args.variant < 2 || args.plain))
+        throw std::invalid_argument("unique-row counting runs on the batched one-CTA-per-query "
+                                    "kernels");
+    a.visit = nullptr;
     if (args.variant >= 2) {
-        const SeismicPlan p = plan_seismic_cta(kind, a.fwd.dim, a.qcap, a.k, n, args, args.plain);
+        SeismicSearchArgs pa = args;
+        if (args.count_unique) {
+            // one stamp per doc per CTA: a grid of one CTA per SM, one query each
+            pa.cluster = 1;
+            pa.max_ctas = device_sm_count();
+        }
+        const SeismicPlan p = plan_seismic_cta(kind, a.fwd.dim, a.qcap, a.k, n, pa, args.plain);
+        if (args.count_unique) {
+            const size_t stamps = static_cast<size_t>(p.blocks) *
+                                  static_cast<size_t>(std::max(a.fwd.n_docs, 1));
+            a.visit = static_cast<uint32_t*>(ws.dev(Workspace::kVisit, stamps * sizeof(uint32_t)));
+            cuda_check(cudaMemsetAsync(a.visit, 0, stamps * sizeof(uint32_t), s), "memset");
+        }
         const int maxb = std::max(ix.max_blocks(), 1);
         a.variant = args.variant;
         a.batch_docs = p.batch_docs;
@@ -769,6 +785,9 @@ void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
         stats->lists_probed = h[kStatListsProbed];
         stats->kernel_ms = ms;
         stats->launches = launches;
+        stats->row_bytes = h[kStatRowBytes];
+        stats->unique_docs = h[kStatUniqueDocs];
+        stats->unique_row_bytes = h[kStatUniqueRowBytes];
     }
     if (timed) {
         cudaEventDestroy(e0);

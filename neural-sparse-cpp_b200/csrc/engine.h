@@ -94,7 +94,7 @@ class Workspace : public Scratch {
 public:
     enum Slot : int {
         kQIndptr, kQIdx, kQVal, kQCode, kOutD, kOutL, kSel, kBScore, kCounter, kStats,
-        kCandD, kCandL, kHeapD, kHeapL, kQValG, kIds, kErr, kOrder, kSortKeys, kNumSlots
+        kCandD, kCandL, kHeapD, kHeapL, kQValG, kIds, kErr, kOrder, kSortKeys, kVisit, kNumSlots
     };
     static Workspace& get();
     cudaStream_t stream() const { return stream_; }
@@ -252,6 +252,9 @@ struct SearchStats {
     unsigned long long lists_probed = 0;
     float kernel_ms = 0.0f;
     int launches = 0;
+    unsigned long long row_bytes = 0;         // rows' share of `bytes`
+    unsigned long long unique_docs = 0;       // counting pass only
+    unsigned long long unique_row_bytes = 0;  // counting pass only
 };
 
 // A SEISMIC kernel launch shape chosen by the autotuner (variant < 0: none).
@@ -288,6 +291,10 @@ struct SeismicSearchArgs {
     // doc), in device memory; replaces the launch-wide selector
     const uint64_t* const* d_sel_q = nullptr;
     int max_ctas = 0;         // cap on the persistent grid's CTAs (0: none)
+    // variants 2-5, batched: count each scored doc's row once per query, as
+    // the reference's visited set does (a slower counting pass: one stamp per
+    // doc per CTA, on a grid of one CTA per SM)
+    bool count_unique = false;
     int32_t nnz_cap = -1;     // entries the query arrays hold (negative: not checked)
 };
 

@@ -51,6 +51,9 @@ void record_stats(const nsp::SearchStats& s) {
     g_last_stats.lists_probed = s.lists_probed;
     g_last_stats.kernel_ms = s.kernel_ms;
     g_last_stats.launches = s.launches;
+    g_last_stats.row_bytes = s.row_bytes;
+    g_last_stats.unique_docs = s.unique_docs;
+    g_last_stats.unique_row_bytes = s.unique_row_bytes;
 }
 
 void fill_padding(idx_t n, int k, float* d, idx_t* l) {
@@ -80,6 +83,7 @@ nsp::SeismicSearchArgs seismic_args(const SearchParameters* p, int k) {
         a.stage_bytes = p->engine.stage_bytes;
         a.batch_docs = p->engine.batch_docs;
         a.cluster = p->engine.ctas_per_query;
+        a.count_unique = p->engine.count_unique;
     }
     return a;
 }

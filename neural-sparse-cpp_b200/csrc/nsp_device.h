@@ -71,12 +71,21 @@ struct QueryView {
 };
 
 // Counters the search kernels accumulate (unsigned long long each).
+// kStatBytes counts every byte a kernel reads, rows included as often as they
+// are scored; kStatRowBytes is the rows' share of it. A doc met again in a
+// later list is scored again (the reference skips it with its visited set,
+// seismic_index.cpp:104-107), so the reference's algorithmic bytes are
+// kStatBytes - kStatRowBytes + kStatUniqueRowBytes, the last counted only by
+// a launch with `visit` stamps (SeismicLaunch).
 enum StatSlot : int {
     kStatDocsScored = 0,
     kStatBlocksVisited = 1,
     kStatBytes = 2,
     kStatListsProbed = 3,
-    kStatCount = 4,
+    kStatRowBytes = 4,
+    kStatUniqueDocs = 5,
+    kStatUniqueRowBytes = 6,
+    kStatCount = 7,
 };
 
 struct SeismicLaunch {
@@ -123,6 +132,11 @@ struct SeismicLaunch {
     // past it is treated as empty and reported through `err`, like a row
     // longer than qcap.
     int32_t nnz_cap;
+    // Counting pass only (variants 2-5), else nullptr: per CTA, one stamp per
+    // doc (n_docs of them); the walk stamps each doc of a visited block with
+    // the CTA's query number and counts a member doc's row the first time
+    // (kStatUniqueDocs / kStatUniqueRowBytes). Zero on entry.
+    uint32_t* visit;
 };
 
 // Doc-ascending postings of an fp32 forward index (the exact search's

@@ -799,6 +799,7 @@ __device__ bool run_query(const SeismicLaunch& a, const WarpSlice<V>& w, float* 
         atomicAdd(a.stats + kStatBlocksVisited, blocks_visited);
         atomicAdd(a.stats + kStatBytes, bytes);
         atomicAdd(a.stats + kStatListsProbed, lists);
+        atomicAdd(a.stats + kStatRowBytes, lane_bytes);
     }
     __syncwarp();
     return ok;

@@ -85,7 +85,8 @@ struct Ctl {
 __host__ __device__ inline size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
 
 struct CtaLayout {
-    size_t tbl, qv, qterm, qraw, cuts, hs, hid, cdoc, coff, clen, csc, segs, cseg, wsum, total;
+    size_t tbl, qv, qterm, qraw, cuts, hs, hid, cdoc, coff, clen, csc, segs, cseg, wsum, cur, uq,
+        total;
 };
 
 // Shared-memory layout of one CTA. The four candidate arrays are contiguous
@@ -108,6 +109,8 @@ __host__ __device__ inline CtaLayout cta_layout(int vsize, int tsize, int dim, i
     L.segs = o;  o += static_cast<size_t>(seg_cap) * sizeof(Seg);
     L.cseg = o;  o += a16(static_cast<size_t>(batch) * 2);
     L.wsum = o;  o += 32 * 4;
+    L.cur = o;   o += 64;  // warp 0's Cursor
+    L.uq = o;    o += 2 * 32 * 4;  // counting pass: warp 0's per-lane unique docs, row bytes
     L.total = o;
     return L;
 }
@@ -446,7 +449,9 @@ __device__ void sort_blocks(const float* bscore, int nb, unsigned long long* key
     __syncthreads();
 }
 
-// Cursor of warp 0 over one list's visiting order.
+// Cursor of warp 0 over one list's visiting order. It lives in shared memory:
+// only warp 0 uses it (its lanes write the same values), and held in every
+// thread's registers it would cost the scoring loop registers.
 struct Cursor {
     int o;            // next position in the visiting order
     bool dead;        // the first list's walk has ended
@@ -791,6 +796,12 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
         }
         __syncthreads();
 
+        // counting pass: this CTA's stamps, and warp 0's per-lane counts
+        uint32_t* uq = reinterpret_cast<uint32_t*>(smem + L.uq);
+        if (a.visit != nullptr && warp == 0) {
+            uq[lane] = 0;
+            uq[32 + lane] = 0;
+        }
         int n = 0;  // heap size (warp 0)
         bool first = true;
         // Counters of this query (32 bits: a query reads far less than 4 GB).
@@ -842,14 +853,16 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                                          a.heap_factor, order, wsum, tid, lane, warp, nwarps);
                 }
                 // 5. batches
-                Cursor cur;
-                cur.o = 0;
-                cur.dead = false;
-                cur.split = false;
-                cur.split_d = 0;
-                cur.split_left = 0;
-                cur.split_blk = 0;
-                cur.split_bs = 0.0f;
+                Cursor& cur = *reinterpret_cast<Cursor*>(smem + L.cur);
+                if (warp == 0) {
+                    cur.o = 0;
+                    cur.dead = false;
+                    cur.split = false;
+                    cur.split_d = 0;
+                    cur.split_left = 0;
+                    cur.split_blk = 0;
+                    cur.split_bs = 0.0f;
+                }
                 for (;;) {
                     if (warp == 0) {
                         int total = 0;
@@ -944,6 +957,23 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                                 }
                             }
                         };
+                        // counting pass: the member docs of a visited block,
+                        // each counted the first time the query meets it
+                        auto count_visits = [&](int t) {
+                            if (a.visit == nullptr) return;
+                            uint32_t* stamp = a.visit + static_cast<size_t>(blockIdx.x) *
+                                                            static_cast<size_t>(a.fwd.n_docs);
+                            const Seg g = segs[t];
+                            for (int j = lane; j < g.cnt; j += 32) {
+                                const int i = g.cand0 + j;
+                                const int32_t d = cdoc[i];
+                                if (d >= 0 && atomicExch(stamp + d, static_cast<uint32_t>(iter)) !=
+                                                  static_cast<uint32_t>(iter)) {
+                                    uq[lane] += 1;
+                                    uq[32 + lane] += 8u + clen[i] * (2 + vsz);
+                                }
+                            }
+                        };
                         auto end_first_list = [&](int from) {
                             for (int t = from; t < nseg; ++t) give_back(t);
                             cur.dead = true;
@@ -977,6 +1007,14 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                             blocks_visited += __popc(__ballot_sync(kFull, taken && head));
                             bytes += 16u * __popc(__ballot_sync(kFull, taken && head)) +
                                      4u * __reduce_add_sync(kFull, taken ? cnt : 0);
+                            if (a.visit != nullptr) {
+                                unsigned tm = __ballot_sync(kFull, taken);
+                                while (tm) {
+                                    const int t = __ffs(tm) - 1;
+                                    tm &= tm - 1;
+                                    count_visits(s + t);
+                                }
+                            }
                             unsigned dm = __ballot_sync(kFull, lane < upto && fail);
                             while (dm) {  // later lists skip a failing block
                                 const int t = __ffs(dm) - 1;
@@ -1008,6 +1046,7 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                                     bytes += 16;
                                 }
                                 bytes += 4u * static_cast<uint32_t>(g.cnt);
+                                count_visits(s);
                                 for (int b = 0; b < g.cnt; b += 32) {
                                     const int j = b + lane;
                                     float sc = 0.0f;
@@ -1078,6 +1117,20 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                 atomicAdd(a.stats + kStatBytes,
                           static_cast<unsigned long long>(bytes) +
                               static_cast<unsigned long long>(static_cast<long long>(row_bytes)));
+                atomicAdd(a.stats + kStatRowBytes,
+                          static_cast<unsigned long long>(static_cast<long long>(row_bytes)));
+            }
+            if (a.visit != nullptr && warp == 0) {
+                uint32_t ud = uq[lane], ub = uq[32 + lane];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    ud += __shfl_xor_sync(kFull, ud, o);
+                    ub += __shfl_xor_sync(kFull, ub, o);
+                }
+                if (lane == 0) {
+                    atomicAdd(a.stats + kStatUniqueDocs, static_cast<unsigned long long>(ud));
+                    atomicAdd(a.stats + kStatUniqueRowBytes, static_cast<unsigned long long>(ub));
+                }
             }
         }
         // restore the all-zero table for the next query

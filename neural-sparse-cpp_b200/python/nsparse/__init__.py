@@ -76,6 +76,7 @@ _sig("nsp_search_params_set_id_selector", _P, _P)
 _sig("nsp_search_params_set_engine", _P, ctypes.c_int, ctypes.c_int)
 _sig("nsp_search_params_set_kernel", _P, ctypes.c_int, ctypes.c_int)
 _sig("nsp_search_params_set_split", _P, ctypes.c_int)
+_sig("nsp_search_params_set_count_unique", _P, ctypes.c_int)
 _sig("nsp_search_params_free", _P)
 _sig("nsp_index_search_device", _P, _I32, _P, _P, _P, _I32, ctypes.c_int, _P, _P, _P, _P)
 _sig("nsp_device_info", ctypes.POINTER(_I32), ctypes.c_char_p, ctypes.c_size_t)
@@ -87,7 +88,9 @@ _sig("nsp_index_autotune", _P, _I32, _P, _P, _P, ctypes.c_int, _P, ctypes.POINTE
 class _Stats(ctypes.Structure):
     _fields_ = [("docs_scored", ctypes.c_uint64), ("blocks_visited", ctypes.c_uint64),
                 ("bytes", ctypes.c_uint64), ("lists_probed", ctypes.c_uint64),
-                ("kernel_ms", ctypes.c_float), ("launches", ctypes.c_int32)]
+                ("kernel_ms", ctypes.c_float), ("launches", ctypes.c_int32),
+                ("row_bytes", ctypes.c_uint64), ("unique_docs", ctypes.c_uint64),
+                ("unique_row_bytes", ctypes.c_uint64)]
 
 
 _sig("nsp_last_search_stats", ctypes.POINTER(_Stats))
@@ -256,6 +259,12 @@ class SearchParameters:
         """Extension: CTAs per query of SEISMIC variants 2-5 (0 auto, 1, or a
         cluster of 2, 4 or 8 CTAs scoring each query together)."""
         _check(_L.nsp_search_params_set_split(self._h, int(ctas_per_query)))
+
+    def set_count_unique(self, on=True):
+        """Extension: a batched SEISMIC search becomes a counting pass (slower,
+        same results) whose stats also count each scored doc's row once per
+        query, as the reference's visited set does."""
+        _check(_L.nsp_search_params_set_count_unique(self._h, int(bool(on))))
 
     def __del__(self):
         h, self._h = getattr(self, "_h", None), None
@@ -455,10 +464,19 @@ def read_index(file_name, io_flags=0):
 class SearchStats:
     docs_scored: int
     blocks_visited: int
-    bytes: int
+    bytes: int             # every byte read, rows as often as scored
     lists_probed: int
     kernel_ms: float
     launches: int
+    row_bytes: int = 0     # the rows' share of `bytes`
+    unique_docs: int = 0   # counting pass only: docs counted once per query
+    unique_row_bytes: int = 0
+
+    @property
+    def reference_bytes(self) -> int:
+        """The reference's algorithmic bytes (each scored row once per query:
+        its visited set); meaningful after a counting pass."""
+        return self.bytes - self.row_bytes + self.unique_row_bytes
 
 
 def last_search_stats() -> SearchStats:
@@ -466,7 +484,7 @@ def last_search_stats() -> SearchStats:
     s = _Stats()
     _check(_L.nsp_last_search_stats(ctypes.byref(s)))
     return SearchStats(s.docs_scored, s.blocks_visited, s.bytes, s.lists_probed, s.kernel_ms,
-                       s.launches)
+                       s.launches, s.row_bytes, s.unique_docs, s.unique_row_bytes)
 
 
 def device_info():

@@ -75,7 +75,7 @@ class Fwd:
         self.dim, self.n, self.indptr, self.indices = dim, n, indptr, indices
 
 
-def oracle_seismic_from_file(path, qs, k, cut, hf, codes=None, sel_bits=None):
+def oracle_seismic_from_file(path, qs, k, cut, hf, codes=None, sel_bits=None, want_stats=False):
     f = O.read_index_file(str(path))
     if f["kind"] == "IDMP":
         f = f["delegate"]
@@ -85,7 +85,7 @@ def oracle_seismic_from_file(path, qs, k, cut, hf, codes=None, sel_bits=None):
     fw = Fwd(f["dim"], v["n"], v["indptr"], v["indices"])
     qv = qs.values if codes is None else codes
     return O.seismic_search(fw, v["values"], A, qs.indptr, qs.indices, qv, k, cut, hf,
-                            sel_bits=sel_bits)
+                            sel_bits=sel_bits, want_stats=want_stats)
 
 
 def recall(L, T):

@@ -481,6 +481,54 @@ def test_seismic_sq16_device_build(tmp_path):
     np.testing.assert_array_equal(Dr[same], D[same])
 
 
+@pytest.mark.parametrize("kind", ["fp32", "sq8", "fp32-selector"])
+def test_counting_pass_counts_each_scored_row_once_per_query(tmp_path, kind):
+    """The kernel scores a doc met again in a later cut list again (the
+    reference skips it with its visited set, seismic_index.cpp:104-107). Its
+    counting pass stamps visited docs: the docs it counts once per query are
+    exactly the oracle's scored docs, the rest of its scored docs are exactly
+    the oracle's revisits, and results do not change."""
+    docs, qs = golden_corpus()
+    path = tmp_path / "c.idx"
+    codes = None
+    if kind == "sq8":
+        vmin, vmax = float(docs.values.min()), float(docs.values.max())
+        ref_file(docs, sq_spec(vmin, vmax), path)
+        codes = O.sq_encode_u8(vmin, vmax, qs.values)
+    else:
+        ref_file(docs, SEISMIC, path)
+    idx = nsparse.read_index(str(path))
+    sel = bits = None
+    if kind == "fp32-selector":
+        keep = np.arange(0, docs.n, 2, dtype=np.int32)
+        sel = nsparse.SetIDSelector(keep)
+        bits = O.bitmap_from_ids(docs.n, keep)
+
+    def params(count):
+        p = nsparse.SeismicSearchParameters(CUT, HF)
+        p.set_kernel(4, 0)
+        if sel is not None:
+            p.set_id_selector(sel)
+        p.set_count_unique(count)
+        return p
+
+    D, L = search(idx, qs, params=params(False))
+    st = nsparse.last_search_stats()
+    D2, L2 = search(idx, qs, params=params(True))
+    st2 = nsparse.last_search_stats()
+    np.testing.assert_array_equal(L2, L)
+    np.testing.assert_array_equal(D2, D)
+    _, Lo, ost = oracle_seismic_from_file(path, qs, K, CUT, HF, codes=codes, sel_bits=bits,
+                                          want_stats=True)
+    np.testing.assert_array_equal(L, Lo)
+    assert st2.unique_docs == int(ost[:, 0].sum())
+    assert st2.docs_scored == st.docs_scored and st2.row_bytes == st.row_bytes
+    if sel is None:
+        assert st2.docs_scored - st2.unique_docs == int(ost[:, 3].sum())
+    assert 0 < st2.unique_row_bytes <= st2.row_bytes < st2.bytes
+    assert st2.reference_bytes == st2.bytes - st2.row_bytes + st2.unique_row_bytes
+
+
 def test_idmap_seismic_returns_external_ids(tmp_path):
     g = golden()
     docs, qs = golden_corpus()
