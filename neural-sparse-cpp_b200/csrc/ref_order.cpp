@@ -56,4 +56,46 @@ void reference_kept_order(const HostCsr& h, const std::vector<int64_t>& post,
     for (auto& th : pool) th.join();
 }
 
+std::vector<uint16_t> reference_summary_kept(const HostCsr& h, const int32_t* docs, size_t n_docs,
+                                             float alpha) {
+    const float* val = reinterpret_cast<const float*>(h.values.data());
+    std::vector<float> acc(static_cast<size_t>(std::max(h.dim, 1)), 0.0F);
+    std::vector<uint8_t> seen(static_cast<size_t>(std::max(h.dim, 1)), 0);
+    std::vector<uint16_t> touched;
+    float sum = 0.0F;
+    for (size_t i = 0; i < n_docs; ++i) {
+        const int32_t d = docs[i];
+        for (int64_t e = h.indptr[d]; e < h.indptr[d + 1]; ++e) {
+            const uint16_t t = h.indices[e];
+            const float v = val[e];
+            if (!seen[t]) {
+                seen[t] = 1;
+                const float first = std::max(0.0F, v);
+                acc[t] = first;
+                touched.push_back(t);
+                sum += first;
+            } else if (v > acc[t]) {
+                sum += v - acc[t];
+                acc[t] = v;
+            }
+        }
+    }
+    std::vector<std::pair<uint16_t, float>> pairs;
+    pairs.reserve(touched.size());
+    for (const uint16_t t : touched) pairs.emplace_back(t, acc[t]);
+    std::ranges::sort(pairs, [](const auto& a, const auto& b) { return a.second > b.second; });
+    float addup = 0.0F;
+    for (size_t j = 0; j < pairs.size(); ++j) {
+        addup += pairs[j].second;
+        if (addup / sum >= alpha) {
+            pairs.erase(pairs.begin() + static_cast<std::ptrdiff_t>(j) + 1, pairs.end());
+            break;
+        }
+    }
+    std::vector<uint16_t> kept;
+    kept.reserve(pairs.size());
+    for (const auto& pr : pairs) kept.push_back(pr.first);
+    return kept;
+}
+
 }  // namespace nsp

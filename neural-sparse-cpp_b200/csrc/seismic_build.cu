@@ -222,7 +222,8 @@ struct AssignArgs {
 };
 
 template <int ESZ>
-__global__ void __launch_bounds__(256) assign_kernel(AssignArgs a) {
+// Two CTAs per SM (the launch below): up to 128 registers a thread.
+__global__ void __launch_bounds__(256, 2) assign_kernel(AssignArgs a) {
     using acc_t = typename std::conditional<ESZ == 4, float, long long>::type;
     __shared__ int32_t s_list;
     __shared__ int32_t s_touched;
@@ -322,7 +323,46 @@ __global__ void __launch_bounds__(256) assign_kernel(AssignArgs a) {
                     else if constexpr (ESZ == 2) v = reinterpret_cast<const uint16_t*>(fval)[rb + e];
                     else v = fval[rb + e];
                 }
-                // doc terms in order (kmeans_utils.cpp:134-145)
+                if constexpr (ESZ != 4) {
+                    // Integer similarities: the products commute, so the
+                    // doc's (term, centroid entry) pairs are taken 32 at a
+                    // time across its terms -- lane f takes pair f, found by
+                    // a search over the lanes' run ends -- instead of one
+                    // term's short run at a time.
+                    int incl = rn;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y = __shfl_up_sync(kFull, incl, o);
+                        if (lane >= o) incl += y;
+                    }
+                    const int tot = __shfl_sync(kFull, incl, 31);
+                    const int excl = incl - rn;
+                    for (int f0 = 0; f0 < tot; f0 += 32) {
+                        const int f = f0 + lane;
+                        int src = 0;  // the first lane whose run ends after pair f
+#pragma unroll
+                        for (int b = 16; b > 0; b >>= 1) {
+                            const int end = __shfl_sync(kFull, incl, src + b - 1);
+                            if (end <= f) src += b;
+                        }
+                        const int32_t s0 = __shfl_sync(kFull, rs, src);
+                        const int32_t ex = __shfl_sync(kFull, excl, src);
+                        const acc_t dv = __shfl_sync(kFull, v, src);
+                        if (f < tot) {
+                            const int32_t pos = s0 + (f - ex);
+                            const int32_t c = ccl[pos];
+                            long long w;
+                            if constexpr (ESZ == 2) w = reinterpret_cast<const uint16_t*>(cw)[pos];
+                            else w = cw[pos];
+                            atomicAdd(reinterpret_cast<unsigned long long*>(sims + c),
+                                      static_cast<unsigned long long>(dv * w));
+                        }
+                    }
+                    __syncwarp();
+                    continue;
+                }
+                // fp32: doc terms in order (kmeans_utils.cpp:134-145), each
+                // product added in the reference's sequence
                 unsigned m = __ballot_sync(kFull, rn > 0);
                 while (m) {
                     const int src = __ffs(m) - 1;
@@ -458,6 +498,19 @@ __global__ void cut_kernel(const uint64_t* pkey_sorted, const int64_t* pair_off,
             }
         }
         keep[b] = k;
+    }
+}
+
+// Blocks whose alpha cut falls inside a run of equal maxima: which of them
+// the reference keeps is its unstable sort's choice (settled on the host).
+__global__ void cut_tie_kernel(const uint64_t* pkey_sorted, const int64_t* pair_off, int64_t nb,
+                               const int32_t* keep, uint8_t* tie) {
+    for (int64_t b = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; b < nb;
+         b += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t s = pair_off[b], n = pair_off[b + 1] - s;
+        const int64_t k = keep[b];
+        tie[b] = (k > 0 && k < n &&
+                  (pkey_sorted[s + k - 1] >> 16) == (pkey_sorted[s + k] >> 16)) ? 1 : 0;
     }
 }
 
@@ -717,7 +770,7 @@ struct SumPool {
     DevArray<uint32_t> eidx, sidx, tkey, tkey2;
     DevArray<float> eval, delta, mass, tval, tval2;
     DevArray<int32_t> boff, entry_block, run_start, pblock, pair_off32, keep, list_koff;
-    DevArray<uint8_t> has_delta, o_val, sort_tmp;
+    DevArray<uint8_t> has_delta, o_val, sort_tmp, tie;
     DevArray<uint64_t> pkey, pkey2;
 };
 
@@ -725,7 +778,8 @@ template <int ESZ>
 void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
                      const DevArray<int64_t>& d_bdp, nsp::SeismicHost& L, int32_t t0, int32_t t1,
                      const std::vector<int64_t>& doc_eoff, const std::vector<int64_t>& blk_e,
-                     float alpha, cudaStream_t s, SumPool& P, DevColumns& out) {
+                     float alpha, cudaStream_t s, SumPool& P, DevColumns& out,
+                     const nsp::HostCsr* host) {
     const int sms = nsp::device_sm_count();
     const int64_t b0 = L.lbp[t0], b1 = L.lbp[t1];
     const int64_t nb = b1 - b0;
@@ -816,6 +870,40 @@ void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
     std::vector<int32_t> h_keep(static_cast<size_t>(nb));
     P.keep.download(h_keep.data(), h_keep.size(), s);
     cuda_check(cudaStreamSynchronize(s), "D2H");
+    if (host != nullptr) {
+        // fp32: where equal maxima straddle the cut, take the reference's
+        // choice -- its kept terms move to the front of the block's pairs
+        // (the count is the same: equal values give equal running sums)
+        P.tie.grow(nb);
+        cut_tie_kernel<<<sms * 4, 128, 0, s>>>(P.pkey2.data(), P.pair_off.data(), nb,
+                                               P.keep.data(), P.tie.data());
+        cuda_check(cudaGetLastError(), "cut_tie_kernel");
+        std::vector<uint8_t> tie(static_cast<size_t>(nb));
+        P.tie.download(tie.data(), tie.size(), s);
+        cuda_check(cudaStreamSynchronize(s), "D2H");
+        for (int64_t b = 0; b < nb; ++b) {
+            if (!tie[b]) continue;
+            const int64_t gb = b0 + b;
+            const std::vector<uint16_t> kept = nsp::reference_summary_kept(
+                *host, L.docs.data() + L.bdp[gb], static_cast<size_t>(L.bdp[gb + 1] - L.bdp[gb]),
+                alpha);
+            const int64_t ps = pair_off[b], pn = pair_off[b + 1] - ps;
+            std::vector<uint64_t> seg(static_cast<size_t>(pn));
+            cuda_check(cudaMemcpyAsync(seg.data(), P.pkey2.data() + ps, seg.size() * 8,
+                                       cudaMemcpyDeviceToHost, s), "D2H");
+            cuda_check(cudaStreamSynchronize(s), "D2H");
+            std::vector<uint8_t> keep_term(65536, 0);
+            for (const uint16_t t : kept) keep_term[t] = 1;
+            std::stable_partition(seg.begin(), seg.end(),
+                                  [&](uint64_t k) { return keep_term[k & 0xffffu] != 0; });
+            h_keep[b] = static_cast<int32_t>(kept.size());
+            cuda_check(cudaMemcpyAsync(P.pkey2.data() + ps, seg.data(), seg.size() * 8,
+                                       cudaMemcpyHostToDevice, s), "H2D");
+            cuda_check(cudaMemcpyAsync(P.keep.data() + b, &h_keep[b], sizeof(int32_t),
+                                       cudaMemcpyHostToDevice, s), "H2D");
+            cuda_check(cudaStreamSynchronize(s), "sync");
+        }
+    }
     std::vector<int64_t> kept_off(static_cast<size_t>(nb) + 1, 0);
     for (int64_t b = 0; b < nb; ++b) kept_off[b + 1] = kept_off[b] + h_keep[b];
     const int64_t n_kept = kept_off[nb];
@@ -1160,7 +1248,7 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
             continue;
         }
         summarize_batch<ESZ>(f, d_docs, d_bdp, L, t0, t1, doc_eoff, blk_e, p.alpha, s, pool,
-                             cols);
+                             cols, ESZ == 4 ? &st.vectors.host : nullptr);
         t0 = t1;
     }
 
