@@ -222,8 +222,7 @@ struct AssignArgs {
 };
 
 template <int ESZ>
-// Two CTAs per SM (the launch below): up to 128 registers a thread.
-__global__ void __launch_bounds__(256, 2) assign_kernel(AssignArgs a) {
+__global__ void __launch_bounds__(256) assign_kernel(AssignArgs a) {
     using acc_t = typename std::conditional<ESZ == 4, float, long long>::type;
     __shared__ int32_t s_list;
     __shared__ int32_t s_touched;
@@ -323,46 +322,7 @@ __global__ void __launch_bounds__(256, 2) assign_kernel(AssignArgs a) {
                     else if constexpr (ESZ == 2) v = reinterpret_cast<const uint16_t*>(fval)[rb + e];
                     else v = fval[rb + e];
                 }
-                if constexpr (ESZ != 4) {
-                    // Integer similarities: the products commute, so the
-                    // doc's (term, centroid entry) pairs are taken 32 at a
-                    // time across its terms -- lane f takes pair f, found by
-                    // a search over the lanes' run ends -- instead of one
-                    // term's short run at a time.
-                    int incl = rn;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const int y = __shfl_up_sync(kFull, incl, o);
-                        if (lane >= o) incl += y;
-                    }
-                    const int tot = __shfl_sync(kFull, incl, 31);
-                    const int excl = incl - rn;
-                    for (int f0 = 0; f0 < tot; f0 += 32) {
-                        const int f = f0 + lane;
-                        int src = 0;  // the first lane whose run ends after pair f
-#pragma unroll
-                        for (int b = 16; b > 0; b >>= 1) {
-                            const int end = __shfl_sync(kFull, incl, src + b - 1);
-                            if (end <= f) src += b;
-                        }
-                        const int32_t s0 = __shfl_sync(kFull, rs, src);
-                        const int32_t ex = __shfl_sync(kFull, excl, src);
-                        const acc_t dv = __shfl_sync(kFull, v, src);
-                        if (f < tot) {
-                            const int32_t pos = s0 + (f - ex);
-                            const int32_t c = ccl[pos];
-                            long long w;
-                            if constexpr (ESZ == 2) w = reinterpret_cast<const uint16_t*>(cw)[pos];
-                            else w = cw[pos];
-                            atomicAdd(reinterpret_cast<unsigned long long*>(sims + c),
-                                      static_cast<unsigned long long>(dv * w));
-                        }
-                    }
-                    __syncwarp();
-                    continue;
-                }
-                // fp32: doc terms in order (kmeans_utils.cpp:134-145), each
-                // product added in the reference's sequence
+                // doc terms in order (kmeans_utils.cpp:134-145)
                 unsigned m = __ballot_sync(kFull, rn > 0);
                 while (m) {
                     const int src = __ffs(m) - 1;
