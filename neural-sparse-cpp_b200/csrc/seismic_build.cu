@@ -210,6 +210,8 @@ struct AssignArgs {
     int32_t* tcnt;          // [dim] per CTA, zero between lists
     int32_t* tstart;        // [dim] per CTA
     int32_t* tcur;          // [dim] per CTA
+    int2* trun;             // [dim] per CTA: (start, count) of the term's centroid
+                            // entries, count zero between lists
     int32_t* touched;       // [max centroid entries] per CTA
     uint16_t* ccl;          // [max centroid entries] per CTA
     uint8_t* cw;            // [max centroid entries * esz] per CTA
@@ -221,9 +223,36 @@ struct AssignArgs {
     int32_t sims_in_smem;  // 1: the similarity rows are in dynamic shared memory
 };
 
+// Similarity accumulators: fp32 for fp32 values; int for uint8 codes (at
+// most 400 products of two codes below 2^16 each, exact), int64 for uint16.
+template <int ESZ>
+using assign_acc_t = typename std::conditional<
+    ESZ == 4, float, typename std::conditional<ESZ == 1, int, long long>::type>::type;
+
+// One centroid entry of a term's run: the centroid and its value.
+template <int ESZ>
+__device__ __forceinline__ void centroid_entry(const uint16_t* ccl, const uint8_t* cw, int32_t k,
+                                               int32_t& c, assign_acc_t<ESZ>& w) {
+    c = ccl[k];
+    if constexpr (ESZ == 4) w = reinterpret_cast<const float*>(cw)[k];
+    else if constexpr (ESZ == 2) w = reinterpret_cast<const uint16_t*>(cw)[k];
+    else w = cw[k];
+}
+
+template <int ESZ>
+__device__ __forceinline__ void add_product(assign_acc_t<ESZ>* sims, int32_t c,
+                                            assign_acc_t<ESZ> dv, assign_acc_t<ESZ> w) {
+    if constexpr (ESZ == 4) sims[c] = __fadd_rn(sims[c], __fmul_rn(dv, w));
+    else sims[c] += dv * w;
+}
+
 template <int ESZ>
 __global__ void __launch_bounds__(256) assign_kernel(AssignArgs a) {
-    using acc_t = typename std::conditional<ESZ == 4, float, long long>::type;
+    using acc_t = assign_acc_t<ESZ>;
+    // centroid entries of one term in flight per lane: a term's run is
+    // loaded kChunks * 32 entries at a time, the next hit term's first
+    // chunk while the current one is applied
+    constexpr int kChunks = 4;
     __shared__ int32_t s_list;
     __shared__ int32_t s_touched;
     __shared__ int32_t s_total;
@@ -234,6 +263,7 @@ __global__ void __launch_bounds__(256) assign_kernel(AssignArgs a) {
     int32_t* tcnt = a.tcnt + static_cast<size_t>(blockIdx.x) * dim;
     int32_t* tstart = a.tstart + static_cast<size_t>(blockIdx.x) * dim;
     int32_t* tcur = a.tcur + static_cast<size_t>(blockIdx.x) * dim;
+    int2* trun = a.trun + static_cast<size_t>(blockIdx.x) * dim;
     int32_t* touched = a.touched + static_cast<size_t>(blockIdx.x) * a.max_centroid_entries;
     uint16_t* ccl = a.ccl + static_cast<size_t>(blockIdx.x) * a.max_centroid_entries;
     uint8_t* cw = a.cw + static_cast<size_t>(blockIdx.x) * a.max_centroid_entries * ESZ;
@@ -278,8 +308,11 @@ __global__ void __launch_bounds__(256) assign_kernel(AssignArgs a) {
         const int32_t nt = s_touched;
         for (int32_t i = threadIdx.x; i < nt; i += blockDim.x) {
             const int32_t term = touched[i];
-            tstart[term] = atomicAdd(&s_total, tcnt[term]);
+            const int32_t cnt = tcnt[term];
+            const int32_t st = atomicAdd(&s_total, cnt);
+            tstart[term] = st;
             tcur[term] = 0;
+            trun[term] = make_int2(st, cnt);
         }
         __syncthreads();
         for (int32_t c = warp; c < nc; c += wpb) {
@@ -312,34 +345,71 @@ __global__ void __launch_bounds__(256) assign_kernel(AssignArgs a) {
             const int64_t rb = static_cast<int64_t>(ri.x) * nsp::kRowAlign;
             for (uint32_t e0 = 0; e0 < ri.y; e0 += 32) {
                 const uint32_t e = e0 + lane;
-                int32_t rs = 0, rn = 0;
+                int2 run = make_int2(0, 0);
                 acc_t v = 0;
                 if (e < ri.y) {
-                    const int32_t term = a.f.idx[rb + e];
-                    rn = tcnt[term];
-                    if (rn > 0) rs = tstart[term];
+                    run = trun[a.f.idx[rb + e]];
                     if constexpr (ESZ == 4) v = reinterpret_cast<const float*>(fval)[rb + e];
                     else if constexpr (ESZ == 2) v = reinterpret_cast<const uint16_t*>(fval)[rb + e];
                     else v = fval[rb + e];
                 }
-                // doc terms in order (kmeans_utils.cpp:134-145)
-                unsigned m = __ballot_sync(kFull, rn > 0);
-                while (m) {
+                // doc terms in order (kmeans_utils.cpp:134-145); a term's
+                // centroids are distinct, so its products commute, and the
+                // warp barrier between terms keeps each similarity's sum in
+                // doc-term order
+                unsigned m = __ballot_sync(kFull, run.y > 0);
+                int32_t nc_[kChunks];
+                acc_t nw[kChunks];
+                int32_t s0 = 0, cnt = 0;
+                acc_t dv = 0;
+                if (m) {
                     const int src = __ffs(m) - 1;
+                    s0 = __shfl_sync(kFull, run.x, src);
+                    cnt = __shfl_sync(kFull, run.y, src);
+                    dv = __shfl_sync(kFull, v, src);
+#pragma unroll
+                    for (int j = 0; j < kChunks; ++j) {
+                        const int32_t k = j * 32 + lane;
+                        nc_[j] = -1;
+                        if (k < cnt) centroid_entry<ESZ>(ccl, cw, s0 + k, nc_[j], nw[j]);
+                    }
+                }
+                while (m) {
                     m &= m - 1;
-                    const int32_t s0 = __shfl_sync(kFull, rs, src);
-                    const int32_t cnt = __shfl_sync(kFull, rn, src);
-                    const acc_t dv = __shfl_sync(kFull, v, src);
-                    for (int32_t k = lane; k < cnt; k += 32) {
-                        const int32_t c = ccl[s0 + k];
-                        if constexpr (ESZ == 4) {
-                            const float w = reinterpret_cast<const float*>(cw)[s0 + k];
-                            sims[c] = __fadd_rn(sims[c], __fmul_rn(dv, w));
-                        } else if constexpr (ESZ == 2) {
-                            sims[c] += dv * static_cast<long long>(reinterpret_cast<const uint16_t*>(cw)[s0 + k]);
-                        } else {
-                            sims[c] += dv * static_cast<long long>(cw[s0 + k]);
+                    int32_t cc[kChunks];
+                    acc_t cwv[kChunks];
+#pragma unroll
+                    for (int j = 0; j < kChunks; ++j) {
+                        cc[j] = nc_[j];
+                        cwv[j] = nw[j];
+                    }
+                    const int32_t cs0 = s0, ccnt = cnt;
+                    const acc_t cdv = dv;
+                    if (m) {
+                        const int src = __ffs(m) - 1;
+                        s0 = __shfl_sync(kFull, run.x, src);
+                        cnt = __shfl_sync(kFull, run.y, src);
+                        dv = __shfl_sync(kFull, v, src);
+#pragma unroll
+                        for (int j = 0; j < kChunks; ++j) {
+                            const int32_t k = j * 32 + lane;
+                            nc_[j] = -1;
+                            if (k < cnt) centroid_entry<ESZ>(ccl, cw, s0 + k, nc_[j], nw[j]);
                         }
+                    }
+#pragma unroll
+                    for (int j = 0; j < kChunks; ++j)
+                        if (cc[j] >= 0) add_product<ESZ>(sims, cc[j], cdv, cwv[j]);
+                    for (int32_t k0 = kChunks * 32; k0 < ccnt; k0 += kChunks * 32) {
+#pragma unroll
+                        for (int j = 0; j < kChunks; ++j) {
+                            const int32_t k = k0 + j * 32 + lane;
+                            cc[j] = -1;
+                            if (k < ccnt) centroid_entry<ESZ>(ccl, cw, cs0 + k, cc[j], cwv[j]);
+                        }
+#pragma unroll
+                        for (int j = 0; j < kChunks; ++j)
+                            if (cc[j] >= 0) add_product<ESZ>(sims, cc[j], cdv, cwv[j]);
                     }
                     __syncwarp();
                 }
@@ -367,7 +437,10 @@ __global__ void __launch_bounds__(256) assign_kernel(AssignArgs a) {
             __syncwarp();
         }
         __syncthreads();
-        for (int32_t i = threadIdx.x; i < nt; i += blockDim.x) tcnt[touched[i]] = 0;
+        for (int32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+            tcnt[touched[i]] = 0;
+            trun[touched[i]] = make_int2(0, 0);
+        }
         __syncthreads();
     }
 }
@@ -1095,16 +1168,30 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
         for (int64_t d = 0; d < n_docs; ++d)
             max_row = std::max<int64_t>(max_row, h.indptr[d + 1] - h.indptr[d]);
         const int64_t max_ce = std::max<int64_t>(1, static_cast<int64_t>(max_nc) * max_row);
-        const int ctas = sms * 2;
         const int wpb = 8;
+        const size_t acc_bytes = sizeof(assign_acc_t<ESZ>);
+        const size_t sims_smem = static_cast<size_t>(wpb) * std::max(max_nc, 1) * acc_bytes;
+        const bool sims_in_smem = sims_smem <= 96u * 1024u;
+        const size_t smem = sims_in_smem ? sims_smem : 0;
+        if (sims_in_smem) cuda_check(nsp::allow_opt_in_smem(assign_kernel<ESZ>), "assign smem");
+        // as many resident CTAs as fit, up to 4 per SM (each list's
+        // similarity rows are walked with its memory round trips exposed,
+        // so resident warps are what hides them)
+        int per_sm = 0;
+        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, assign_kernel<ESZ>,
+                                                                 wpb * 32, smem),
+                   "assign occupancy");
+        const int ctas = sms * std::max(1, std::min(per_sm, 4));
         DevArray<int32_t> tcnt(static_cast<size_t>(ctas) * dim), tstart(static_cast<size_t>(ctas) * dim),
             tcur(static_cast<size_t>(ctas) * dim), touched(static_cast<size_t>(ctas) * max_ce);
+        DevArray<int2> trun(static_cast<size_t>(ctas) * dim);
         DevArray<uint16_t> ccl(static_cast<size_t>(ctas) * max_ce);
         DevArray<uint8_t> cw(static_cast<size_t>(ctas) * max_ce * ESZ);
         DevArray<uint8_t> isc(static_cast<size_t>(ctas) * std::max<int64_t>(max_kept, 1));
         DevArray<uint8_t> sims(static_cast<size_t>(ctas) * wpb * std::max(max_nc, 1) * 8);
         DevArray<int32_t> work(1);
         cuda_check(cudaMemsetAsync(tcnt.data(), 0, tcnt.size() * 4, s), "memset");
+        cuda_check(cudaMemsetAsync(trun.data(), 0, trun.size() * sizeof(int2), s), "memset");
         cuda_check(cudaMemsetAsync(work.data(), 0, 4, s), "memset");
         AssignArgs a{};
         a.f = f;
@@ -1118,6 +1205,7 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
         a.tcnt = tcnt.data();
         a.tstart = tstart.data();
         a.tcur = tcur.data();
+        a.trun = trun.data();
         a.touched = touched.data();
         a.ccl = ccl.data();
         a.cw = cw.data();
@@ -1126,14 +1214,7 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
         a.max_centroid_entries = max_ce;
         a.max_kept = std::max<int64_t>(max_kept, 1);
         a.max_nc = std::max(max_nc, 1);
-        const size_t acc_bytes = ESZ == 4 ? 4 : 8;
-        const size_t sims_smem = static_cast<size_t>(wpb) * a.max_nc * acc_bytes;
-        size_t smem = 0;
-        if (sims_smem <= 96u * 1024u) {
-            cuda_check(nsp::allow_opt_in_smem(assign_kernel<ESZ>), "assign smem");
-            a.sims_in_smem = 1;
-            smem = sims_smem;
-        }
+        a.sims_in_smem = sims_in_smem ? 1 : 0;
         assign_kernel<ESZ><<<ctas, wpb * 32, smem, s>>>(a);
         cuda_check(cudaGetLastError(), "assign_kernel");
         cuda_check(cudaStreamSynchronize(s), "assign sync");
