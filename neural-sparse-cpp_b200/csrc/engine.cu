@@ -745,7 +745,7 @@ void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
         a.bcap = p.bcap;
         const size_t warps = static_cast<size_t>(p.blocks) * p.wpb;
         a.bscore = static_cast<float*>(
-            ws.dev(Workspace::kBScore, warps * a.ix.max_blocks * sizeof(float)));
+            ws.dev(Workspace::kBScore, warps * one_warp_slot(a.ix.max_blocks) * sizeof(float)));
         a.work_counter = static_cast<int32_t*>(ws.dev(Workspace::kCounter, sizeof(int32_t)));
         cuda_check(cudaMemsetAsync(a.work_counter, 0, sizeof(int32_t), s), "memset");
         a.first_query = 0;
@@ -762,7 +762,8 @@ void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
         a.variant = p.variant;
         a.stage_bytes = p.stage_bytes;
         a.bcap = p.bcap;
-        a.bscore = static_cast<float*>(ws.dev(Workspace::kBScore, a.ix.max_blocks * sizeof(float)));
+        a.bscore = static_cast<float*>(
+            ws.dev(Workspace::kBScore, one_warp_slot(a.ix.max_blocks) * sizeof(float)));
         a.work_counter = nullptr;
         mark(e0);
         for (int32_t q = 0; q < n; ++q) {
@@ -819,7 +820,7 @@ SeismicScratchNeed seismic_scratch_need(const ForwardDevice& fwd, const SeismicD
     } else {
         const int words = (fwd.view().dim + 31) / 32;
         const SeismicPlan p = plan_seismic(kind, words, qcap, args.k, n, args, ix.max_blocks());
-        need.per_cta = static_cast<size_t>(p.wpb) * ix.max_blocks() * sizeof(float);
+        need.per_cta = static_cast<size_t>(p.wpb) * one_warp_slot(ix.max_blocks()) * sizeof(float);
         need.ctas = p.blocks;
         need.cluster = 1;
     }

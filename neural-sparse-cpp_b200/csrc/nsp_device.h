@@ -88,6 +88,13 @@ enum StatSlot : int {
     kStatCount = 7,
 };
 
+// One-warp kernels (variants 0-1): floats per warp of `bscore` -- the
+// current list's block scores, then the first list's (score, block) pairs
+// sorted into the reference's visiting order (8 bytes each).
+__host__ __device__ inline size_t one_warp_slot(int max_blocks) {
+    return 3 * static_cast<size_t>((max_blocks + 1) & ~1);
+}
+
 struct SeismicLaunch {
     FwdView fwd;
     SeismicView ix;
@@ -101,7 +108,8 @@ struct SeismicLaunch {
     int32_t* out_l;
     int32_t qcap;               // max query nnz in the batch
     int32_t* work_counter;      // work stealing over queries, or nullptr
-    float* bscore;              // scratch: per warp slot, max_blocks floats
+    float* bscore;              // scratch: per warp slot (one_warp_slot floats for
+                                // variants 0-1; wpb * max_blocks per CTA otherwise)
     unsigned long long* stats;  // kStatCount counters, or nullptr
     int32_t first_query;        // static mode: queries first_query.. strided
     // Variant 1 (staged): doc rows arrive in shared memory by bulk copy,

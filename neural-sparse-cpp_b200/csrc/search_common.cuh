@@ -7,6 +7,8 @@
 
 #include <cstdint>
 
+#include "ref_ranking.cuh"
+
 namespace nsp {
 namespace detail_search {
 
@@ -27,45 +29,60 @@ struct ValT<uint16_t> {
     __device__ static float f(uint16_t v) { return static_cast<float>(v); }
 };
 
-// Sorted (score desc, id asc) array of size n <= k in shared memory. A full
-// heap rejects score <= its minimum (utils/ranker.h:58-60) and otherwise drops
-// its worst entry (ranker.h:67-71). A doc already present is not inserted
-// twice. All lanes of the warp call with the same arguments.
+// A query entry's weight as the reference's TopKHolder sees it (a float).
+template <typename V>
+struct QueryWeight {
+    const V* q;
+    __host__ __device__ float operator()(uint16_t i) const { return static_cast<float>(q[i]); }
+};
+
+// The query's top-k holder in shared memory: the reference's TopKHolder
+// (utils/ranker.h:34-138), a binary heap with the smallest score on top
+// (hs[0], hid[0]), restated in ref_ranking.cuh. A full holder rejects
+// score <= its top; otherwise a full holder pops, then pushes. A doc already
+// held is not offered twice (the reference never offers a doc twice: its
+// visited set; a doc offered again here scored at most the top when it was
+// dropped or rejected, and the top only grows). All lanes of the warp call
+// with the same arguments; lane 0 moves the entries.
 __device__ __forceinline__ void heap_offer(float s, int32_t d, float* hs, int32_t* hid,
                                            int& n, int k, int lane) {
-    if (n == k && !(s > hs[k - 1])) return;
+    if (n >= k && s <= hs[0]) return;
     bool found = false;
     for (int i = lane; i < n; i += 32) found |= (hid[i] == d);
     if (__any_sync(kFull, found)) return;
-    int cnt = 0;
-    for (int i = lane; i < n; i += 32) {
-        const float a = hs[i];
-        cnt += (a > s || (a == s && hid[i] < d)) ? 1 : 0;
-    }
-    const int pos = static_cast<int>(__reduce_add_sync(kFull, static_cast<unsigned>(cnt)));
-    const int newn = n < k ? n + 1 : k;
-    for (int hi = newn - 1; hi > pos; hi -= 32) {
-        const int j = hi - lane;
-        const bool act = j > pos;
-        float tv = 0.0f;
-        int32_t ti = 0;
-        if (act) {
-            tv = hs[j - 1];
-            ti = hid[j - 1];
-        }
-        __syncwarp();
-        if (act) {
-            hs[j] = tv;
-            hid[j] = ti;
-        }
-        __syncwarp();
-    }
     if (lane == 0) {
-        hs[pos] = s;
-        hid[pos] = d;
+        int m = n;
+        ranking::topk_add(ranking::TopK{hs, hid}, m, k, s, d);
     }
     __syncwarp();
-    n = newn;
+    n = n < k ? n + 1 : k;
+}
+
+// The holder's smallest score (valid when it holds k entries).
+__device__ __forceinline__ float heap_top(const float* hs) { return hs[0]; }
+
+// Results as TopKHolder::top_k_items_descending gives them (ranker.h:
+// 113-127), padded with (-1.0, -1) to k (seismic_index.cpp:270-273); scores
+// times `scale` when it is not 0 (SQ decode,
+// seismic_scalar_quantized_index.cpp:345-355). Empties the holder. Lane 0
+// pops; all lanes pad.
+__device__ __forceinline__ void heap_emit(float* hs, int32_t* hid, int n, int k, float scale,
+                                          float* od, int32_t* ol, int lane) {
+    if (lane == 0) {
+        int m = n;
+        const ranking::TopK h{hs, hid};
+        for (int i = n - 1; i >= 0; --i) {
+            const float s = hs[0];
+            od[i] = scale != 0.0f ? __fmul_rn(s, scale) : s;
+            ol[i] = hid[0];
+            ranking::topk_pop(h, m);
+        }
+    }
+    for (int i = n + lane; i < k; i += 32) {
+        od[i] = -1.0f;
+        ol[i] = -1;
+    }
+    __syncwarp();
 }
 
 }  // namespace detail_search

@@ -37,6 +37,7 @@
 namespace nsp {
 namespace {
 
+using detail_search::heap_emit;
 using detail_search::heap_offer;
 using detail_search::kFull;
 using detail_search::ValT;
@@ -638,22 +639,18 @@ __device__ bool run_query(const SeismicLaunch& a, const WarpSlice<V>& w, float* 
             run += __popc(w.qbits[i]);
         }
     }
-    // 2. query cut: value desc, position asc; original order if cut >= nnz
+    // 2. query cut (utils/vector_process.h:18-30): the query's order when
+    // cut >= nnz, else the reference's TopKHolder over (value, position)
     int ncut;
     if (a.cut >= qn) {
         ncut = qn;
         for (int i = lane; i < qn; i += 32) w.cuts[i] = w.qterm[i];
     } else {
         ncut = a.cut;
-        for (int i = lane; i < qn; i += 32) {
-            const float vi = ValT<V>::f(w.qval[i]);
-            int rank = 0;
-            for (int j = 0; j < qn; ++j) {
-                const float vj = ValT<V>::f(w.qval[j]);
-                rank += (vj > vi || (vj == vi && j < i)) ? 1 : 0;
-            }
-            if (rank < ncut) w.cuts[rank] = w.qterm[i];
-        }
+        if (lane == 0)
+            ranking::cut_like_reference(w.cuts, qn, ncut, detail_search::QueryWeight<V>{w.qval});
+        __syncwarp();
+        for (int i = lane; i < ncut; i += 32) w.cuts[i] = w.qterm[w.cuts[i]];
     }
     __syncwarp();
 
@@ -711,39 +708,22 @@ __device__ bool run_query(const SeismicLaunch& a, const WarpSlice<V>& w, float* 
             }
             // 4. block traversal
             if (first) {
-                for (;;) {
-                    float bs = -FLT_MAX;
-                    int bb = INT_MAX;
-                    for (int b = lane; b < nb; b += 32) {
-                        const float s = bscore[b];
-                        if (s == -INFINITY) continue;  // already visited
-                        if (bb == INT_MAX || s > bs || (s == bs && b < bb)) {
-                            bs = s;
-                            bb = b;
-                        }
-                    }
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) {
-                        const float s2 = __shfl_xor_sync(kFull, bs, o);
-                        const int b2 = __shfl_xor_sync(kFull, bb, o);
-                        if (b2 != INT_MAX &&
-                            (bb == INT_MAX || s2 > bs || (s2 == bs && b2 < bb))) {
-                            bs = s2;
-                            bb = b2;
-                        }
-                    }
-                    if (bb == INT_MAX) break;
-                    if (n == a.k && __fmul_rn(bs, a.heap_factor) < w.hs[a.k - 1]) break;
-                    __syncwarp();
-                    if (lane == 0) bscore[bb] = -INFINITY;
-                    __syncwarp();
+                // the reference's visiting order (seismic_common.h:105-115)
+                ranking::Blk* items = reinterpret_cast<ranking::Blk*>(
+                    bscore_g + ((a.ix.max_blocks + 1) & ~1));
+                for (int b = lane; b < nb; b += 32) items[b] = ranking::Blk{bscore[b], b};
+                __syncwarp();
+                ranking::warp_sort_blocks_like_reference(items, nb, lane);
+                for (int o = 0; o < nb; ++o) {
+                    const ranking::Blk it = items[o];
+                    if (n == a.k && __fmul_rn(it.s, a.heap_factor) < w.hs[0]) break;
                     ++blocks_visited;
                     if constexpr (kStaged) {
-                        ok = visit_block_staged<V>(a, w, lb0 + bb, n, lane, phase_bits, docs_scored,
-                                                   bytes, lane_bytes);
+                        ok = visit_block_staged<V>(a, w, lb0 + it.b, n, lane, phase_bits,
+                                                   docs_scored, bytes, lane_bytes);
                         if (!ok) break;
                     } else {
-                        visit_block<V>(a, w, lb0 + bb, n, lane, docs_scored, bytes, lane_bytes);
+                        visit_block<V>(a, w, lb0 + it.b, n, lane, docs_scored, bytes, lane_bytes);
                     }
                 }
             } else {
@@ -751,13 +731,13 @@ __device__ bool run_query(const SeismicLaunch& a, const WarpSlice<V>& w, float* 
                     const int b = b0 + lane;
                     const float s = b < nb ? bscore[b] : 0.0f;
                     const bool cand =
-                        b < nb && !(n == a.k && __fmul_rn(s, a.heap_factor) < w.hs[a.k - 1]);
+                        b < nb && !(n == a.k && __fmul_rn(s, a.heap_factor) < w.hs[0]);
                     unsigned cm = __ballot_sync(kFull, cand);
                     while (cm) {
                         const int src = __ffs(cm) - 1;
                         cm &= cm - 1;
                         const float S = __shfl_sync(kFull, s, src);
-                        if (n == a.k && __fmul_rn(S, a.heap_factor) < w.hs[a.k - 1]) continue;
+                        if (n == a.k && __fmul_rn(S, a.heap_factor) < w.hs[0]) continue;
                         ++blocks_visited;
                         if constexpr (kStaged) {
                             ok = visit_block_staged<V>(a, w, lb0 + b0 + src, n, lane, phase_bits,
@@ -779,18 +759,8 @@ __device__ bool run_query(const SeismicLaunch& a, const WarpSlice<V>& w, float* 
 
     // 6. results, padded with (-1.0, -1); SQ scores decoded
     //    (seismic_scalar_quantized_index.cpp:345-355).
-    float* od = a.out_d + static_cast<size_t>(q) * a.k;
-    int32_t* ol = a.out_l + static_cast<size_t>(q) * a.k;
-    for (int i = lane; i < a.k; i += 32) {
-        if (i < n) {
-            const float s = w.hs[i];
-            od[i] = a.decode_scale != 0.0f ? __fmul_rn(s, a.decode_scale) : s;
-            ol[i] = w.hid[i];
-        } else {
-            od[i] = -1.0f;
-            ol[i] = -1;
-        }
-    }
+    heap_emit(w.hs, w.hid, n, a.k, a.decode_scale, a.out_d + static_cast<size_t>(q) * a.k,
+              a.out_l + static_cast<size_t>(q) * a.k, lane);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) lane_bytes += __shfl_xor_sync(kFull, lane_bytes, o);
     bytes += lane_bytes;
@@ -816,7 +786,7 @@ __global__ void __launch_bounds__(256) seismic_search_kernel(SeismicLaunch a) {
     WarpSlice<V> w = carve<V>(smem + per * warp, a.ix.words, a.qcap, a.k, bcap, sb);
     const int wpb = blockDim.x >> 5;
     const int gw = blockIdx.x * wpb + warp;
-    float* bscore = a.bscore + static_cast<size_t>(gw) * a.ix.max_blocks;
+    float* bscore = a.bscore + static_cast<size_t>(gw) * one_warp_slot(a.ix.max_blocks);
     uint32_t phase_bits = 0;
     if constexpr (kStaged) {
         if (lane == 0) {
@@ -901,17 +871,8 @@ __global__ void __launch_bounds__(32) exact_list_kernel(FwdView fwd, QueryView q
         for (int i = 0; i < cnt; ++i) heap_offer(w.csc[i], w.cdoc[i], w.hs, w.hid, n, k, lane);
         __syncwarp();
     }
-    for (int i = lane; i < k; i += 32) {
-        const size_t o = static_cast<size_t>(q) * k + i;
-        if (i < n) {
-            const float s = w.hs[i];
-            out_d[o] = decode_scale != 0.0f ? __fmul_rn(s, decode_scale) : s;
-            out_l[o] = w.hid[i];
-        } else {
-            out_d[o] = -1.0f;
-            out_l[o] = -1;
-        }
-    }
+    heap_emit(w.hs, w.hid, n, k, decode_scale, out_d + static_cast<size_t>(q) * k,
+              out_l + static_cast<size_t>(q) * k, lane);
 }
 
 // ------------------------------------------------------- quantize (SQ) --

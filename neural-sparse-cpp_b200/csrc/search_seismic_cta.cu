@@ -55,6 +55,8 @@ namespace nsp {
 namespace {
 
 namespace cg = cooperative_groups;
+using detail_search::heap_emit;
+using detail_search::QueryWeight;
 using detail_search::heap_offer;
 using detail_search::kFull;
 using detail_search::ValT;
@@ -444,38 +446,19 @@ __device__ void list_summaries(const SeismicLaunch& a, int t, int nb, const uint
     }
 }
 
-// Sort key: ascending key order = score descending, block ascending. +0.0
-// and -0.0 compare equal, as the reference's comparator has them.
-__device__ __forceinline__ unsigned long long order_key(float s, int b) {
-    uint32_t u = __float_as_uint(s == 0.0f ? 0.0f : s);
-    u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);  // ascending with s
-    return (static_cast<unsigned long long>(~u) << 32) | static_cast<uint32_t>(b);
-}
-
-// Bitonic sort of the first list's blocks; writes the visiting order.
-__device__ void sort_blocks(const float* bscore, int nb, unsigned long long* keys, int p2,
-                            uint16_t* order, int tid, int nthreads) {
-    for (int i = tid; i < p2; i += nthreads)
-        keys[i] = i < nb ? order_key(__ldcg(bscore + i), i) : ~0ull;
-    __syncthreads();
-    for (int k2 = 2; k2 <= p2; k2 <<= 1) {
-        for (int j = k2 >> 1; j > 0; j >>= 1) {
-            for (int i = tid; i < p2; i += nthreads) {
-                const int ixj = i ^ j;
-                if (ixj > i) {
-                    const unsigned long long x = keys[i];
-                    const unsigned long long y = keys[ixj];
-                    const bool up = (i & k2) == 0;
-                    if ((x > y) == up) {
-                        keys[i] = y;
-                        keys[ixj] = x;
-                    }
-                }
-            }
-            __syncthreads();
-        }
+// The first list's visiting order: the reference's std::ranges::sort of the
+// block indices by summary score descending (seismic_common.h:105-115),
+// restated in ref_ranking.cuh -- equal scores keep the order the reference's
+// unstable sort leaves. Warp 0 sorts (score, block) pairs in `items`; the
+// other warps wait at the barrier.
+__device__ void sort_blocks(const float* bscore, int nb, ranking::Blk* items, uint16_t* order,
+                            int tid, int warp, int lane) {
+    if (warp == 0) {
+        for (int i = lane; i < nb; i += 32) items[i] = ranking::Blk{__ldcg(bscore + i), i};
+        __syncwarp();
+        ranking::warp_sort_blocks_like_reference(items, nb, lane);
+        for (int i = lane; i < nb; i += 32) order[i] = static_cast<uint16_t>(items[i].b);
     }
-    for (int i = tid; i < nb; i += nthreads) order[i] = static_cast<uint16_t>(keys[i] & 0xffffu);
     __syncthreads();
 }
 
@@ -524,7 +507,7 @@ __device__ int gather(const SeismicLaunch& a, Cursor& c, bool first, int64_t lb0
         if (c.split_left == 0) c.split = false;
     }
     const bool full = n == a.k;
-    const float hmin = full ? hs[a.k - 1] : 0.0f;
+    const float hmin = full ? hs[0] : 0.0f;
     while (!c.split && !c.dead && room > 0 && nseg < seg_cap && c.o < nb) {
         const int p = c.o + lane;
         const bool in = p < nb;
@@ -807,22 +790,17 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
         }
         const bool nonfinite = __syncthreads_or(bad) != 0;
 
-        // 2. query cut: value desc, position asc; original order if cut >= nnz
+        // 2. query cut (utils/vector_process.h:18-30): the query's order when
+        // cut >= nnz, else the reference's TopKHolder over (value, position)
         int ncut;
         if (a.cut >= qn) {
             ncut = qn;
             for (int i = tid; i < qn; i += blockDim.x) cuts[i] = qterm[i];
         } else {
             ncut = a.cut;
-            for (int i = tid; i < qn; i += blockDim.x) {
-                const float vi = ValT<V>::f(qraw[i]);
-                int rank = 0;
-                for (int j = 0; j < qn; ++j) {
-                    const float vj = ValT<V>::f(qraw[j]);
-                    rank += (vj > vi || (vj == vi && j < i)) ? 1 : 0;
-                }
-                if (rank < ncut) cuts[rank] = qterm[i];
-            }
+            if (tid == 0) ranking::cut_like_reference(cuts, qn, ncut, QueryWeight<V>{qraw});
+            __syncthreads();
+            for (int i = tid; i < ncut; i += blockDim.x) cuts[i] = qterm[cuts[i]];
         }
         __syncthreads();
 
@@ -869,17 +847,16 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                 if (first) {
                     int p2 = 1;
                     while (p2 < nb) p2 <<= 1;
-                    unsigned long long* keys = p2 <= 2 * batch
-                                                   ? reinterpret_cast<unsigned long long*>(cdoc)
-                                                   : keys_g;
-                    if (keys == nullptr) {  // the host sizes sortkeys; never taken
+                    ranking::Blk* items = reinterpret_cast<ranking::Blk*>(
+                        p2 <= 2 * batch ? reinterpret_cast<unsigned long long*>(cdoc) : keys_g);
+                    if (items == nullptr) {  // the host sizes sortkeys; never taken
                         if (tid == 0) atomicExch(a.err, 2);
                         break;
                     }
-                    sort_blocks(bscore, nb, keys, p2, order, tid, blockDim.x);
+                    sort_blocks(bscore, nb, items, order, tid, warp, lane);
                 } else {
                     const int nh = ctl->nheap;
-                    nbv = passing_blocks(bscore, nb, nh == a.k, nh == a.k ? hs[a.k - 1] : 0.0f,
+                    nbv = passing_blocks(bscore, nb, nh == a.k, nh == a.k ? hs[0] : 0.0f,
                                          a.heap_factor, order, wsum, tid, lane, warp, nwarps);
                 }
                 // 5. batches
@@ -957,13 +934,13 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                     // grows); segments holding such docs are flagged.
                     {
                         const int nh = ctl->nheap;
-                        const float hmin0 = nh == a.k ? hs[a.k - 1] : 0.0f;
+                        const float hmin0 = nh == a.k ? hs[0] : 0.0f;
                         for (int i = tid; i < total; i += blockDim.x) {
                             if (cdoc[i] >= 0) {
                                 ++docs_scored;
                                 row_bytes += 8 + static_cast<int32_t>(clen[i]) * (2 + vsz);
                                 // a flag: every writer stores the same 1
-                                if (nh < a.k || csc[i] > hmin0) segs[cseg[i]].surv = 1;
+                                if (nh < a.k || !(csc[i] <= hmin0)) segs[cseg[i]].surv = 1;
                             }
                         }
                         __syncthreads();
@@ -1027,7 +1004,7 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                             const unsigned sm = __ballot_sync(kFull, valid && surv > 0);
                             const int S = sm ? __ffs(sm) - 1 : w;  // first that may change the heap
                             const bool full = n == a.k;
-                            const float hmin = full ? hs[a.k - 1] : 0.0f;
+                            const float hmin = full ? hs[0] : 0.0f;
                             const bool fail =
                                 lane < S && head && full && __fmul_rn(bs, a.heap_factor) < hmin;
                             const unsigned fm = __ballot_sync(kFull, fail);
@@ -1062,7 +1039,7 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                             // segment s holds survivors: its test, then its offers
                             const Seg g = segs[s];
                             if (g.head && n == a.k &&
-                                __fmul_rn(g.bs, a.heap_factor) < hs[a.k - 1]) {
+                                __fmul_rn(g.bs, a.heap_factor) < hs[0]) {
                                 if (first) {
                                     end_first_list(s);
                                     ended = true;
@@ -1086,7 +1063,7 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
                                         sc = csc[g.cand0 + j];
                                     }
                                     unsigned m = __ballot_sync(
-                                        kFull, d >= 0 && (n < a.k || sc > hs[a.k - 1]));
+                                        kFull, d >= 0 && (n < a.k || !(sc <= hs[0])));
                                     while (m) {
                                         const int src = __ffs(m) - 1;
                                         m &= m - 1;
@@ -1111,20 +1088,9 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
         }
         // results, padded with (-1.0, -1); SQ scores decoded
         // (seismic_scalar_quantized_index.cpp:345-355)
-        if (warp == 0) {
-            float* od = a.out_d + static_cast<size_t>(q) * a.k;
-            int32_t* ol = a.out_l + static_cast<size_t>(q) * a.k;
-            for (int i = lane; i < a.k; i += 32) {
-                if (i < n) {
-                    const float s = hs[i];
-                    od[i] = a.decode_scale != 0.0f ? __fmul_rn(s, a.decode_scale) : s;
-                    ol[i] = hid[i];
-                } else {
-                    od[i] = -1.0f;
-                    ol[i] = -1;
-                }
-            }
-        }
+        if (warp == 0)
+            heap_emit(hs, hid, n, a.k, a.decode_scale, a.out_d + static_cast<size_t>(q) * a.k,
+                      a.out_l + static_cast<size_t>(q) * a.k, lane);
         if (a.stats != nullptr) {
             // per warp: its threads' doc counts and row bytes, plus its
             // summary bytes (the same on every lane) and, for warp 0, the

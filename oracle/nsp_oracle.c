@@ -59,6 +59,78 @@ static void topk_emit(const topk_t* h, float* d, int32_t* l) {
     }
 }
 
+/* ---- the reference's TopKHolder for SEISMIC: utils/ranker.h:34-138 -------
+ * A std::priority_queue with std::greater on the score: a binary heap with the
+ * smallest score at a[0]. The sift steps are the C++ library's push_heap /
+ * pop_heap (bits/stl_heap.h: __push_heap, __adjust_heap), which decide which
+ * of several equal scores is dropped and in which order equal scores leave. */
+
+typedef struct {
+    item_t* a; /* binary heap, smallest score on top */
+    int n, k;
+} rheap_t;
+
+static void rh_sift_up(item_t* a, int hole, item_t v) {
+    int parent = (hole - 1) / 2;
+    while (hole > 0 && a[parent].s > v.s) {
+        a[hole] = a[parent];
+        hole = parent;
+        parent = (hole - 1) / 2;
+    }
+    a[hole] = v;
+}
+
+static void rh_sift_down(item_t* a, int len, item_t v) {
+    int hole = 0, child = 0;
+    while (child < (len - 1) / 2) {
+        child = 2 * (child + 1);
+        if (a[child].s > a[child - 1].s) --child;
+        a[hole] = a[child];
+        hole = child;
+    }
+    if ((len & 1) == 0 && child == (len - 2) / 2) {
+        child = 2 * (child + 1);
+        a[hole] = a[child - 1];
+        hole = child - 1;
+    }
+    rh_sift_up(a, hole, v);
+}
+
+static void rh_pop(rheap_t* h) {
+    if (h->n > 1) {
+        item_t v = h->a[h->n - 1];
+        h->a[h->n - 1] = h->a[0];
+        rh_sift_down(h->a, h->n - 1, v);
+    }
+    h->n--;
+}
+
+/* TopKHolder::add (ranker.h:58-72) */
+static void rh_add(rheap_t* h, float s, int32_t id) {
+    item_t v;
+    if (h->n >= h->k && s <= h->a[0].s) return;
+    if (h->n >= h->k) rh_pop(h);
+    v.s = s;
+    v.id = id;
+    rh_sift_up(h->a, h->n, v);
+    h->n++;
+}
+
+/* top_k_items_descending (ranker.h:113-127), padded with (-1.0, -1)
+ * (seismic_index.cpp:270-273); empties the heap. */
+static void rh_emit(rheap_t* h, float* d, int32_t* l) {
+    const int n = h->n;
+    for (int i = n - 1; i >= 0; --i) {
+        d[i] = h->a[0].s;
+        l[i] = h->a[0].id;
+        rh_pop(h);
+    }
+    for (int i = n; i < h->k; ++i) {
+        d[i] = -1.0f;
+        l[i] = -1;
+    }
+}
+
 static inline int sel_member(const uint64_t* bits, int32_t d) {
     return bits == NULL || ((bits[d >> 6] >> (d & 63)) & 1u);
 }
@@ -161,24 +233,22 @@ int nspo_cut(const uint16_t* idx, const void* vals, int esz, int len, int cut,
         for (int i = 0; i < len; ++i) out[i] = idx[i];
         return len;
     }
-    /* rank by (value desc, position asc): O(len*cut) selection, taken mask */
-    unsigned char* taken = (unsigned char*)calloc((size_t)len, 1);
-    if (!taken) return -1;
-    for (int r = 0; r < cut; ++r) {
-        int best = -1;
-        float bv = 0.0f;
-        for (int i = 0; i < len; ++i) {
-            if (taken[i]) continue;
-            float vi = val_at(vals, esz, i);
-            if (best < 0 || vi > bv) {
-                best = i;
-                bv = vi;
-            }
+    /* a TopKHolder of size cut offered (value, term) in query order, then
+     * top_k_descending: the heap's pops fill the result from its end */
+    {
+        item_t* hp = (item_t*)malloc(sizeof(item_t) * (size_t)cut);
+        rheap_t h;
+        if (!hp) return -1;
+        h.a = hp;
+        h.n = 0;
+        h.k = cut;
+        for (int i = 0; i < len; ++i) rh_add(&h, val_at(vals, esz, i), (int32_t)idx[i]);
+        for (int i = h.n - 1; i >= 0; --i) {
+            out[i] = (uint16_t)h.a[0].id;
+            rh_pop(&h);
         }
-        taken[best] = 1;
-        out[r] = idx[best];
+        free(hp);
     }
-    free(taken);
     return cut;
 }
 
@@ -198,12 +268,131 @@ typedef struct {
     int32_t b;
 } blk_t;
 
-static int blk_cmp(const void* x, const void* y) {
-    const blk_t* a = (const blk_t*)x;
-    const blk_t* b = (const blk_t*)y;
-    if (a->s > b->s) return -1;
-    if (a->s < b->s) return 1;
-    return a->b - b->b;
+/* reorder_clusters (seismic_common.h:105-115): std::ranges::sort of the block
+ * indices by score descending -- the C++ library's introsort
+ * (bits/stl_algo.h: __introsort_loop, __unguarded_partition_pivot,
+ * __final_insertion_sort; heap sort past the depth budget), whose steps
+ * decide where equal scores land. */
+static int blk_before(blk_t x, blk_t y) { return x.s > y.s; }
+
+static void blk_swap(blk_t* a, int64_t i, int64_t j) {
+    blk_t t = a[i];
+    a[i] = a[j];
+    a[j] = t;
+}
+
+static void blk_heap_up(blk_t* a, int64_t hole, int64_t top, blk_t v) {
+    int64_t parent = (hole - 1) / 2;
+    while (hole > top && blk_before(a[parent], v)) {
+        a[hole] = a[parent];
+        hole = parent;
+        parent = (hole - 1) / 2;
+    }
+    a[hole] = v;
+}
+
+static void blk_heap_adjust(blk_t* a, int64_t hole, int64_t len, blk_t v) {
+    const int64_t top = hole;
+    int64_t child = hole;
+    while (child < (len - 1) / 2) {
+        child = 2 * (child + 1);
+        if (blk_before(a[child], a[child - 1])) child--;
+        a[hole] = a[child];
+        hole = child;
+    }
+    if ((len & 1) == 0 && child == (len - 2) / 2) {
+        child = 2 * (child + 1);
+        a[hole] = a[child - 1];
+        hole = child - 1;
+    }
+    blk_heap_up(a, hole, top, v);
+}
+
+static void blk_heap_sort(blk_t* a, int64_t len) {
+    if (len < 2) return;
+    for (int64_t parent = (len - 2) / 2;; parent--) {
+        blk_heap_adjust(a, parent, len, a[parent]);
+        if (parent == 0) break;
+    }
+    while (len > 1) {
+        blk_t v;
+        len--;
+        v = a[len];
+        a[len] = a[0];
+        blk_heap_adjust(a, 0, len, v);
+    }
+}
+
+static void blk_introsort(blk_t* a, int64_t f, int64_t l, int depth) {
+    while (l - f > 16) {
+        int64_t mid, lo, hi;
+        blk_t piv;
+        if (depth == 0) {
+            blk_heap_sort(a + f, l - f);
+            return;
+        }
+        depth--;
+        /* median of a[f+1], a[mid], a[l-1] to the front */
+        mid = f + (l - f) / 2;
+        if (blk_before(a[f + 1], a[mid])) {
+            if (blk_before(a[mid], a[l - 1])) blk_swap(a, f, mid);
+            else if (blk_before(a[f + 1], a[l - 1])) blk_swap(a, f, l - 1);
+            else blk_swap(a, f, f + 1);
+        } else if (blk_before(a[f + 1], a[l - 1])) {
+            blk_swap(a, f, f + 1);
+        } else if (blk_before(a[mid], a[l - 1])) {
+            blk_swap(a, f, l - 1);
+        } else {
+            blk_swap(a, f, mid);
+        }
+        piv = a[f];
+        lo = f + 1;
+        hi = l;
+        for (;;) {
+            while (blk_before(a[lo], piv)) lo++;
+            hi--;
+            while (blk_before(piv, a[hi])) hi--;
+            if (!(lo < hi)) break;
+            blk_swap(a, lo, hi);
+            lo++;
+        }
+        blk_introsort(a, lo, l, depth);
+        l = lo;
+    }
+}
+
+static void blk_linear_insert(blk_t* a, int64_t i) {
+    blk_t v = a[i];
+    while (blk_before(v, a[i - 1])) {
+        a[i] = a[i - 1];
+        i--;
+    }
+    a[i] = v;
+}
+
+static void blk_insertion(blk_t* a, int64_t f, int64_t l) {
+    for (int64_t i = f + 1; i < l; ++i) {
+        if (blk_before(a[i], a[f])) {
+            blk_t v = a[i];
+            memmove(a + f + 1, a + f, (size_t)(i - f) * sizeof(blk_t));
+            a[f] = v;
+        } else {
+            blk_linear_insert(a, i);
+        }
+    }
+}
+
+static void blk_sort_like_reference(blk_t* a, int64_t n) {
+    int lg = 0;
+    if (n <= 0) return;
+    while ((n >> (lg + 1)) > 0) lg++;
+    blk_introsort(a, 0, n, 2 * lg);
+    if (n > 16) {
+        blk_insertion(a, 0, 16);
+        for (int64_t i = 16; i < n; ++i) blk_linear_insert(a, i);
+    } else {
+        blk_insertion(a, 0, n);
+    }
 }
 
 int nspo_seismic_search(int dim, int esz, int32_t n_docs, const int32_t* d_indptr,
@@ -251,7 +440,7 @@ int nspo_seismic_search(int dim, int esz, int32_t n_docs, const int32_t* d_indpt
                 else dense8[qi[i]] = q8[i];
             }
             int ncut = nspo_cut(qi, qany, esz, qlen, cut, cuts);
-            topk_t h = {buf, 0, k};
+            rheap_t h = {buf, 0, k};
             int64_t n_scored = 0, n_blk_visit = 0, n_blk_seen = 0, n_revisit = 0;
             int first = 1;
             for (int c = 0; c < ncut; ++c) {
@@ -281,13 +470,13 @@ int nspo_seismic_search(int dim, int esz, int32_t n_docs, const int32_t* d_indpt
                         }
                     }
                     /* reorder_clusters: seismic_common.h:105-115 */
-                    if (first) qsort(blocks, (size_t)nb, sizeof(blk_t), blk_cmp);
+                    if (first) blk_sort_like_reference(blocks, nb);
                     /* query_single_inverted_list: seismic_index.cpp:78-117 */
                     for (int64_t o = 0; o < nb; ++o) {
                         const float bs = blocks[o].s;
                         const int64_t b = b0 + blocks[o].b;
                         ++n_blk_seen;
-                        if (h.n == h.k && bs * heap_factor < h.a[h.n - 1].s) {
+                        if (h.n == h.k && bs * heap_factor < h.a[0].s) {
                             if (first) break;
                             continue;
                         }
@@ -324,13 +513,13 @@ int nspo_seismic_search(int dim, int esz, int32_t n_docs, const int32_t* d_indpt
                                 s = (float)acc;
                             }
                             ++n_scored;
-                            topk_add(&h, s, d);
+                            rh_add(&h, s, d);
                         }
                     }
                 }
                 first = 0; /* seismic_index.cpp:261: set after every list */
             }
-            topk_emit(&h, out_d + (int64_t)q * k, out_l + (int64_t)q * k);
+            rh_emit(&h, out_d + (int64_t)q * k, out_l + (int64_t)q * k);
             if (stats) {
                 stats[(int64_t)q * 4 + 0] = n_scored;
                 stats[(int64_t)q * 4 + 1] = n_blk_visit;

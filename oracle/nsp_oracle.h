@@ -4,16 +4,20 @@
  * Plain-C restatement of the reference's search hot path
  * (opensearch-project/neural-sparse-cpp). Only tests/, __graft_entry__.smoke()
  * and bench.py's CPU-baseline leg load it. Each function names the reference
- * file:line it restates. Where the reference leaves an order unspecified (ties
- * in std::priority_queue and in its unstable std::ranges::sort calls), this
- * oracle fixes one total order, the same one the device kernels use:
- *   - result ranking: score descending, then doc id ascending;
- *   - a full top-k heap rejects a score <= its minimum (utils/ranker.h:58-72)
- *     and evicts its worst entry (lowest score, then highest id);
- *   - query cut: value descending, then position ascending, and the original
- *     order when cut >= nnz (utils/vector_process.h:18-30);
- *   - first-list block order: summary score descending, then block id
- *     ascending (seismic_common.h:105-115).
+ * file:line it restates. Where the reference's order of equal values comes
+ * from its std::priority_queue (TopKHolder, utils/ranker.h) and its unstable
+ * std::ranges::sort, SEISMIC search follows the C++ library's own steps for
+ * them, as the device kernels do:
+ *   - the query cut: a TopKHolder of size cut over (value, term) in query
+ *     order, popped into top_k_descending order; the query's own order when
+ *     cut >= nnz (utils/vector_process.h:18-30);
+ *   - the first list's blocks: std::ranges::sort by summary score descending
+ *     (seismic_common.h:105-115), the library's introsort;
+ *   - the results: a TopKHolder (rejects score <= its top; pops, then pushes)
+ *     drained by top_k_items_descending (seismic_index.cpp:263-273).
+ * Exact search (BrutalIndex, InvertedIndex) fixes one total order instead:
+ * score descending, then doc id ascending; a full top-k rejects a score <= its
+ * minimum and evicts its worst entry (lowest score, then highest id).
  * Pinned by tests/test_oracle.py against the reference library compiled from
  * its sources (oracle/_ref) and against fixtures under tests/golden/.
  */
