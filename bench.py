@@ -527,12 +527,10 @@ def sq_workload(docs, qs, hf=SQ_HF, cut=SQ_CUT):
 
 def row_parity(D, L, Dr, Lr):
     """Engine rows against the reference's rows for the same queries and
-    index file. A row is tied when its engine scores repeat a value (the order
-    of equal scores is left unspecified by the reference). A doc both return
-    must carry the same score in both (common-pair mismatches); rows may still
-    differ where ties in block scores change the reference's visiting order
-    (its unstable sort, seismic_common.h:105-115), so the overlap of the two
-    result sets is reported too."""
+    index file: identical rows (ids, their order and scores), and separately
+    the rows whose scores repeat a value (their order is the reference's
+    top-k holder's, which the engine follows), the scores of docs both return
+    (common-pair mismatches) and the overlap of the two result sets."""
     same = (L == Lr).all(axis=1) & (D == Dr).all(axis=1)
     tied = np.array([len(set(d[l >= 0].tolist())) < int((l >= 0).sum()) for d, l in zip(D, L)])
     same_scores = (np.sort(D, axis=1) == np.sort(Dr, axis=1)).all(axis=1)
