@@ -474,16 +474,24 @@ __global__ void entries_kernel(nsp::FwdView f, const int32_t* docs, const int64_
 // One thread per (block, term) run of the term-sorted entries: the running max
 // gives each entry's increment of the block mass (inverted_list_clusters.cpp:
 // 96-114); the run's final max becomes a candidate summary pair.
+// uint8 codes: a block's mass is a sum of integer increments below 2^24, so
+// every order of the float additions gives the same value -- the sum of its
+// terms' maxima. Each run adds its max to the block's integer mass instead
+// of writing per-entry increments for the ordered sum.
 template <int ESZ>
 __global__ void runs_kernel(const uint16_t* skey, const uint32_t* sidx, const float* eval,
                             const int32_t* run_start, int64_t n_runs, int64_t n_entries,
                             const int32_t* entry_block, float* delta, uint8_t* has_delta,
-                            uint64_t* pkey, int32_t* pblock) {
+                            uint64_t* pkey, int32_t* pblock, uint32_t* mass_u) {
     for (int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; r < n_runs;
          r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const int64_t s = run_start[r];
         const int64_t e = r + 1 < n_runs ? run_start[r + 1] : n_entries;
         float acc = 0.0f;
+        if constexpr (ESZ == 1) {
+            for (int64_t i = s; i < e; ++i) acc = fmaxf(acc, eval[sidx[i]]);
+            atomicAdd(mass_u + entry_block[sidx[s]], static_cast<uint32_t>(acc));
+        } else {
         for (int64_t i = s; i < e; ++i) {
             const uint32_t oi = sidx[i];
             const float v = eval[oi];
@@ -500,6 +508,7 @@ __global__ void runs_kernel(const uint16_t* skey, const uint32_t* sidx, const fl
             } else {
                 has_delta[oi] = 0;
             }
+        }
         }
         const uint32_t term = skey[s];
         // sort key for the alpha cut: value descending, term ascending
@@ -644,6 +653,12 @@ __global__ void block_first_run_kernel(const int64_t* pos, const int32_t* boff, 
     for (int64_t b = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; b < nb;
          b += static_cast<int64_t>(gridDim.x) * blockDim.x)
         first_run[b] = boff[b] < ne ? pos[boff[b]] : n_runs;
+}
+
+__global__ void mass_from_int_kernel(const uint32_t* mass_u, int64_t nb, float* mass) {
+    for (int64_t b = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; b < nb;
+         b += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        mass[b] = static_cast<float>(mass_u[b]);
 }
 
 __global__ void mass_kernel(const float* delta, const uint8_t* has_delta, const int32_t* boff,
@@ -800,7 +815,7 @@ struct SumPool {
     DevArray<int64_t> doc_eoff, flag, pos, first_run, pair_off, kept_off, rflag, rpos, o_start,
         o_lcol;
     DevArray<uint16_t> ekey, skey, block_local, o_blk, o_term;
-    DevArray<uint32_t> eidx, sidx, tkey, tkey2;
+    DevArray<uint32_t> eidx, sidx, tkey, tkey2, mass_u;
     DevArray<float> eval, delta, mass, tval, tval2;
     DevArray<int32_t> boff, entry_block, run_start, pblock, pair_off32, keep, list_koff;
     DevArray<uint8_t> has_delta, o_val, sort_tmp, tie;
@@ -874,20 +889,32 @@ void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
         for (int64_t b = nb - 1; b >= 0; --b)
             if (boff64[b] == boff64[b + 1]) pair_off[b] = pair_off[b + 1];
     }
-    P.delta.grow(ne);
-    P.has_delta.grow(ne);
+    if constexpr (ESZ != 1) {
+        P.delta.grow(ne);
+        P.has_delta.grow(ne);
+    }
     P.pkey.grow(nr1);
     P.pkey2.grow(nr1);
     P.pblock.grow(nr1);
+    P.mass.grow(nb);
+    if constexpr (ESZ == 1) {
+        P.mass_u.grow(nb);
+        cuda_check(cudaMemsetAsync(P.mass_u.data(), 0, static_cast<size_t>(nb) * 4, s), "memset");
+    }
     runs_kernel<ESZ><<<sms * 8, 256, 0, s>>>(P.skey.data(), P.sidx.data(), P.eval.data(),
                                              P.run_start.data(), n_runs, ne,
                                              P.entry_block.data(), P.delta.data(),
-                                             P.has_delta.data(), P.pkey.data(), P.pblock.data());
+                                             P.has_delta.data(), P.pkey.data(), P.pblock.data(),
+                                             ESZ == 1 ? P.mass_u.data() : nullptr);
     cuda_check(cudaGetLastError(), "runs_kernel");
-    P.mass.grow(nb);
-    mass_kernel<<<sms * 4, 128, 0, s>>>(P.delta.data(), P.has_delta.data(), P.boff.data(), nb,
-                                        P.mass.data());
-    cuda_check(cudaGetLastError(), "mass_kernel");
+    if constexpr (ESZ == 1) {
+        mass_from_int_kernel<<<sms * 4, 256, 0, s>>>(P.mass_u.data(), nb, P.mass.data());
+        cuda_check(cudaGetLastError(), "mass_from_int_kernel");
+    } else {
+        mass_kernel<<<sms * 4, 128, 0, s>>>(P.delta.data(), P.has_delta.data(), P.boff.data(), nb,
+                                            P.mass.data());
+        cuda_check(cudaGetLastError(), "mass_kernel");
+    }
     g_steps.mark("runs, mass");
     // alpha cut over each block's maxima, value descending
     const std::vector<int32_t> pair_off32 = to_i32_offsets(pair_off);
