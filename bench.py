@@ -1,26 +1,27 @@
-"""Benchmark: SEISMIC FP32 search at 1M docs (the reference's shape: SPLADE
-vectors over the 30,522-term BERT vocabulary), queries per second.
+"""Benchmark of the sparse-search hot path, queries per second.
 
-Workload (synthetic, seeded; stands in for MS MARCO SPLADE): 1,000,000 docs
-with lognormal nnz (median 110, clipped 10-400), 10,000 queries (median 25,
-clipped 3-120), Zipf(1.1) terms without replacement, lognormal(0, 0.8) values.
-Index: seismic, lambda=4000 (posting cap), beta=400 (blocks per list =
-0.1 * lambda), alpha=0.4, seed=7, built on the GPU. Search: cut=10,
-heap_factor=0.8, k=10.
+Default workload (`--workload sq8-8.8m`, the headline): SEISMIC-SQ search with
+8-bit codes (per-index min/max scale) over 8,800,000 synthetic docs (the shape
+of MS MARCO SPLADE: lognormal nnz median 120 over the 30,522-term BERT vocab,
+Zipf(1.1) terms, lognormal(0, 0.8) values; seeded, not the dataset), built on
+the GPU with lambda=6000, beta=600, alpha=0.4, seed=7; 65,536 queries of 5-200
+terms per step in four launches of 16,384; cut 12, heap factor 0.9, k=10.
+`value` times the device-resident step (CUDA-graph replays, queries and
+results in HBM); `e2e` times the same queries through `Index.search` with host
+buffers (copies inside the timed region). The index (~4 GB) exceeds L2, and L2
+is also flushed between timed steps.
 
-A step is one batched search of the 10,000 queries (one persistent kernel
-launch). `value` times the device-resident call (queries and results in HBM);
-`e2e` times the host-buffer call (the reference-facing API: pinned H2D of the
-queries, search, D2H of the results). The index (~5 GB) exceeds L2, and L2 is
-also flushed between timed steps.
+Other workloads: `fp32-1m` (SEISMIC fp32, 1M docs, 10,000 queries, lambda 4000,
+beta 400, alpha 0.4, cut 10, heap factor 0.8), `brutal-100k` (exact brute
+force), `build-1m` (the device build beside the reference's GPU-offload build).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-  python bench.py --docs 300000 --queries 4000 --kernel-only --variant 2
-      (a smaller case of the same workload, search launches only: the
-      profiling case; --variant/--tuning pick the search kernel)
+  python bench.py --docs 3000000 --queries 16384 --kernel-only --no-graph --variant 4
+      (a smaller case of the headline, search launches only: the profiling
+      case; --variant/--tuning pick the search kernel)
 
 Under torchrun each rank is a replica holding the whole index and searching
-its own 10,000 queries (weak scaling, no collective on the data path).
+its own queries (weak scaling, no collective on the data path).
 """
 
 from __future__ import annotations

@@ -26,6 +26,10 @@
 //                   are sorted by value descending (term ascending on ties)
 //                   and cut where the running mass reaches alpha (:37-65),
 //                   then transposed term-major per list (:230-293).
+//                   uint8 codes take a fused path (section 5'): per block in
+//                   shared memory, the maxima in a hash or per-term table,
+//                   the integer mass and the cut from a histogram of the
+//                   maxima, no sort of the entries.
 // The lists come back to the host for persistence and are uploaded in the
 // search layout.
 #include <cub/device/device_segmented_sort.cuh>
@@ -811,6 +815,476 @@ __global__ void column_bounds_kernel(const int64_t* start, int64_t n_cols, int64
 
 // Device buffers of the summary pipeline, kept across batches of lists (they
 // only grow), so a batch allocates and frees nothing.
+// ------------------------------------------- 5'. uint8 summaries, fused --
+// With uint8 codes a block's summary needs no ordered arithmetic: its mass is
+// the integer sum of its terms' maxima (below 2^24, so every float sum of
+// them is exact), and the alpha cut over the maxima sorted by (value desc,
+// term asc) follows from a 256-bin histogram of the maxima: the level at
+// which the running sum first reaches alpha * mass, and how many of that
+// level's terms -- the smallest term ids -- are kept. Each block is summed up
+// in shared memory without sorting its entries: blocks of up to
+// kSumHashEntries entries by a CTA of kSumHashThreads threads over a hash
+// table of (term, max), larger blocks by a CTA with a per-term table. A
+// count pass gives each block's kept pairs, a write pass writes them (in no
+// particular order: the per-list transpose sorts them by term and block).
+
+constexpr int kSumSlotsLog = 12;
+constexpr int kSumSlots = 1 << kSumSlotsLog;  // hash slots per CTA
+constexpr int kSumHashEntries = 3072;         // <= 3/4 of the slots: probes stay short
+constexpr int kSumHashThreads = 128;
+constexpr int kSumDenseThreads = 512;
+constexpr int kSumTieScratch = 512;           // tied terms ranked in shared memory
+
+struct SumU8Args {
+    nsp::FwdView f;
+    const int32_t* docs;  // every block's docs, block after block
+    const int64_t* bdp;   // [n_blocks + 1]
+    const int64_t* ids;   // the blocks this launch sums up (global ids), ascending
+    int64_t n_ids;
+    float alpha;
+    int32_t* keep;        // count pass: kept pairs per block (global id)
+    // write pass: block b's pairs go to kept_off[b - b0] + 0.. as
+    // tkey = term << 16 | block_local[b - b0], tval = value
+    const int64_t* kept_off;
+    const uint16_t* block_local;
+    int64_t b0;
+    uint32_t* tkey;
+    float* tval;
+};
+
+struct SumCut {
+    int keep;   // pairs kept
+    int vstar;  // the level the cut falls in (-1: every pair is kept)
+    int r;      // that level's pairs kept (its smallest terms)
+};
+
+// The alpha cut (inverted_list_clusters.cpp:43-51) from the histogram of a
+// block's maxima, by one warp: walking the pairs by value descending, the
+// first count whose running sum `addup` satisfies addup / sum >= alpha. The
+// running sums are integers below 2^24, so (float) of each is the reference's
+// float accumulation; the division is the same correctly rounded one. No
+// such count (sum 0, or alpha above 1): every pair is kept.
+__device__ SumCut sum_u8_cut(const uint32_t* hist, uint32_t mass, int n_pairs, float alpha,
+                             int lane) {
+    uint32_t c[8];
+    uint32_t cs = 0, ss = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int v = 255 - 8 * lane - i;  // lane 0 holds the top levels
+        c[i] = hist[v];
+        cs += c[i];
+        ss += c[i] * static_cast<uint32_t>(v);
+    }
+    // counts and sums of the levels above this lane's
+    uint32_t ci = cs, si = ss;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t cu = __shfl_up_sync(kFull, ci, o);
+        const uint32_t su = __shfl_up_sync(kFull, si, o);
+        if (lane >= o) {
+            ci += cu;
+            si += su;
+        }
+    }
+    uint32_t cnt_above = ci - cs, sum_above = si - ss;
+    const float fm = static_cast<float>(mass);
+    int found = -1;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const uint32_t v = static_cast<uint32_t>(255 - 8 * lane - i);
+        if (found < 0 && c[i] > 0) {
+            const uint32_t end = sum_above + c[i] * v;
+            if (__fdiv_rn(static_cast<float>(end), fm) >= alpha) {
+                found = i;
+            } else {
+                sum_above = end;
+                cnt_above += c[i];
+            }
+        }
+    }
+    const unsigned hit = __ballot_sync(kFull, found >= 0);
+    SumCut out{n_pairs, -1, 0};
+    if (hit == 0u) return out;
+    const int src = __ffs(hit) - 1;
+    int keep = 0, vstar = 0, r = 0;
+    if (lane == src) {
+        uint32_t cf = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            if (i == found) cf = c[i];
+        const uint32_t v = static_cast<uint32_t>(255 - 8 * lane - found);
+        // the smallest j in [1, cf] whose sum satisfies the test (the test
+        // only turns true as j grows)
+        uint32_t lo = 1, hi = cf;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__fdiv_rn(static_cast<float>(sum_above + mid * v), fm) >= alpha)
+                hi = mid;
+            else
+                lo = mid + 1;
+        }
+        keep = static_cast<int>(cnt_above + lo);
+        vstar = static_cast<int>(v);
+        r = static_cast<int>(lo);
+    }
+    out.keep = __shfl_sync(kFull, keep, src);
+    out.vstar = __shfl_sync(kFull, vstar, src);
+    out.r = __shfl_sync(kFull, r, src);
+    return out;
+}
+
+// Position of this lane's item among the warp's `pred` items appended to
+// *counter (every lane of the warp calls it).
+__device__ __forceinline__ int warp_append(unsigned* counter, bool pred, int lane) {
+    const unsigned m = __ballot_sync(kFull, pred);
+    if (m == 0u) return -1;
+    const int leader = __ffs(m) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(counter, static_cast<unsigned>(__popc(m)));
+    base = __shfl_sync(kFull, base, leader);
+    return pred ? static_cast<int>(base + __popc(m & ((1u << lane) - 1u))) : -1;
+}
+
+// One row's 8 elements per lane from element e (rows start on 64-element
+// boundaries and are padded to them, so the 16- and 8-byte loads are aligned
+// and inside the row's padding).
+__device__ __forceinline__ void row8(const nsp::FwdView& f, int64_t rb, int e, uint32_t (&t)[4],
+                                     uint2& c) {
+    const uint4 tv = __ldg(reinterpret_cast<const uint4*>(f.idx + rb + e));
+    t[0] = tv.x;
+    t[1] = tv.y;
+    t[2] = tv.z;
+    t[3] = tv.w;
+    c = __ldg(reinterpret_cast<const uint2*>(static_cast<const uint8_t*>(f.val) + rb + e));
+}
+
+__device__ __forceinline__ uint32_t term8(const uint32_t (&t)[4], int u) {
+    return (u & 1) ? (t[u >> 1] >> 16) : (t[u >> 1] & 0xffffu);
+}
+
+__device__ __forceinline__ uint32_t code8(const uint2& c, int u) {
+    return ((u < 4 ? c.x : c.y) >> (8 * (u & 3))) & 0xffu;
+}
+
+// Writes the kept pairs of block b. `pair_at(i)` gives pair i of the block's
+// nu pairs as (term << 8 | value); ties at the cut level are ranked by term
+// in `tied` (scratch of kSumTieScratch terms) or, when more, against all pairs.
+template <class PairAt>
+__device__ void sum_u8_write(const SumU8Args& a, int64_t b, int nu, const SumCut& cut,
+                             uint32_t ntied, PairAt pair_at, uint16_t* tied, unsigned* s_out,
+                             unsigned* s_ntied, int tid, int nthreads) {
+    const int lane = tid & 31;
+    const int64_t out0 = a.kept_off[b - a.b0];
+    const uint32_t bl = a.block_local[b - a.b0];
+    const bool partial = cut.vstar >= 0 && static_cast<uint32_t>(cut.r) < ntied;
+    const bool scratch = ntied <= static_cast<uint32_t>(kSumTieScratch);
+    for (int base = 0; base < nu; base += nthreads) {
+        const int i = base + tid;
+        uint32_t p = 0;
+        if (i < nu) p = pair_at(i);
+        const int v = static_cast<int>(p & 0xffu);
+        const uint32_t t = p >> 8;
+        const bool kept = i < nu && (cut.vstar < 0 || v > cut.vstar || (v == cut.vstar && !partial));
+        const int o = warp_append(s_out, kept, lane);
+        if (kept) {
+            a.tkey[out0 + o] = (t << 16) | bl;
+            a.tval[out0 + o] = static_cast<float>(v);
+        }
+        const bool tie = partial && scratch && i < nu && v == cut.vstar;
+        const int q = warp_append(s_ntied, tie, lane);
+        if (tie) tied[q] = static_cast<uint16_t>(t);
+    }
+    __syncthreads();
+    if (!partial) return;
+    if (scratch) {
+        for (int base = 0; base < static_cast<int>(ntied); base += nthreads) {
+            const int i = base + tid;
+            bool take = false;
+            uint32_t t = 0;
+            if (i < static_cast<int>(ntied)) {
+                t = tied[i];
+                int rank = 0;
+                for (uint32_t j = 0; j < ntied; ++j) rank += tied[j] < t ? 1 : 0;
+                take = rank < cut.r;
+            }
+            const int o = warp_append(s_out, take, lane);
+            if (take) {
+                a.tkey[out0 + o] = (t << 16) | bl;
+                a.tval[out0 + o] = static_cast<float>(cut.vstar);
+            }
+        }
+    } else {
+        for (int base = 0; base < nu; base += nthreads) {
+            const int i = base + tid;
+            bool take = false;
+            uint32_t t = 0;
+            if (i < nu) {
+                const uint32_t p = pair_at(i);
+                t = p >> 8;
+                if (static_cast<int>(p & 0xffu) == cut.vstar) {
+                    int rank = 0;
+                    for (int j = 0; j < nu; ++j) {
+                        const uint32_t q = pair_at(j);
+                        rank += (static_cast<int>(q & 0xffu) == cut.vstar && (q >> 8) < t) ? 1 : 0;
+                    }
+                    take = rank < cut.r;
+                }
+            }
+            const int o = warp_append(s_out, take, lane);
+            if (take) {
+                a.tkey[out0 + o] = (t << 16) | bl;
+                a.tval[out0 + o] = static_cast<float>(cut.vstar);
+            }
+        }
+    }
+}
+
+// Blocks of at most kSumHashEntries entries: (term + 1) << 8 | max in an
+// open-addressing table of kSumSlots words; warp w takes the block's docs
+// w, w + 4, ..., 8 row elements per lane per step.
+template <bool kWrite>
+__global__ void __launch_bounds__(kSumHashThreads) sum_u8_hash_kernel(SumU8Args a) {
+    __shared__ uint32_t tab[kSumSlots];
+    __shared__ uint32_t hist[256];
+    __shared__ uint16_t uslot[kSumHashEntries];
+    __shared__ unsigned s_nu, s_out, s_ntied;
+    __shared__ uint32_t s_mass;
+    __shared__ SumCut s_cut;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int kWarps = kSumHashThreads / 32;
+    for (int i = tid; i < kSumSlots; i += kSumHashThreads) tab[i] = 0u;
+    for (int i = tid; i < 256; i += kSumHashThreads) hist[i] = 0u;
+    for (int64_t j = blockIdx.x; j < a.n_ids; j += gridDim.x) {
+        const int64_t b = a.ids[j];
+        if (tid == 0) {
+            s_nu = 0u;
+            s_out = 0u;
+            s_ntied = 0u;
+            s_mass = 0u;
+        }
+        __syncthreads();
+        // 1. per-term maxima (inverted_list_clusters.cpp:89-115: the first
+        // value of a term is max(0, v), a uint8 code is never below 0)
+        const int64_t d0 = a.bdp[b], d1 = a.bdp[b + 1];
+        for (int64_t d = d0 + warp; d < d1; d += kWarps) {
+            const uint2 ri = __ldg(a.f.rowinfo + a.docs[d]);
+            const int64_t rb = static_cast<int64_t>(ri.x) * nsp::kRowAlign;
+            const int len = static_cast<int>(ri.y);
+            for (int e0 = 0; e0 < len; e0 += 256) {
+                const int e = e0 + 8 * lane;
+                uint32_t tw[4] = {0u, 0u, 0u, 0u};
+                uint2 cw = make_uint2(0u, 0u);
+                if (e < len) row8(a.f, rb, e, tw, cw);
+                unsigned nnew = 0u;
+                uint32_t slots[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    slots[u] = 0xffffffffu;
+                    if (e + u < len) {
+                        const uint32_t t = term8(tw, u);
+                        const uint32_t key = ((t + 1u) << 8) | code8(cw, u);
+                        uint32_t h = (t * 0x9E3779B1u) >> (32 - kSumSlotsLog);
+                        // at most kSumHashEntries keys in kSumSlots slots:
+                        // an empty slot or the term's own is always found
+                        for (int p = 0; p < kSumSlots; ++p) {
+                            const uint32_t old = atomicCAS(&tab[h], 0u, key);
+                            if (old == 0u) {
+                                slots[u] = h;
+                                ++nnew;
+                                break;
+                            }
+                            if ((old >> 8) == t + 1u) {
+                                if ((old & 0xffu) < (key & 0xffu)) atomicMax(&tab[h], key);
+                                break;
+                            }
+                            h = (h + 1u) & (kSumSlots - 1);
+                        }
+                    }
+                }
+                // new slots appended to the block's list
+                unsigned incl = nnew;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const unsigned x = __shfl_up_sync(kFull, incl, o);
+                    if (lane >= o) incl += x;
+                }
+                unsigned base = 0u;
+                const unsigned total = __shfl_sync(kFull, incl, 31);
+                if (lane == 31 && total > 0u) base = atomicAdd(&s_nu, total);
+                base = __shfl_sync(kFull, base, 31) + incl - nnew;
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (slots[u] != 0xffffffffu) uslot[base++] = static_cast<uint16_t>(slots[u]);
+            }
+        }
+        __syncthreads();
+        // 2. mass and histogram of the maxima
+        const int nu = static_cast<int>(s_nu);
+        uint32_t m = 0u;
+        for (int i = tid; i < nu; i += kSumHashThreads) {
+            const uint32_t v = tab[uslot[i]] & 0xffu;
+            m += v;
+            atomicAdd(&hist[v], 1u);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m += __shfl_xor_sync(kFull, m, o);
+        if (lane == 0 && m > 0u) atomicAdd(&s_mass, m);
+        __syncthreads();
+        // 3. the cut
+        if (warp == 0) {
+            const SumCut c = sum_u8_cut(hist, s_mass, nu, a.alpha, lane);
+            if (lane == 0) s_cut = c;
+        }
+        __syncthreads();
+        const SumCut cut = s_cut;
+        if constexpr (!kWrite) {
+            if (tid == 0) a.keep[b] = cut.keep;
+        } else {
+            const uint32_t ntied = cut.vstar >= 0 ? hist[cut.vstar] : 0u;
+            __syncthreads();  // the histogram becomes the tie scratch
+            sum_u8_write(
+                a, b, nu, cut, ntied,
+                [&](int i) {
+                    const uint32_t k = tab[uslot[i]];
+                    return (((k >> 8) - 1u) << 8) | (k & 0xffu);
+                },
+                reinterpret_cast<uint16_t*>(hist), &s_out, &s_ntied, tid, kSumHashThreads);
+        }
+        __syncthreads();
+        // 4. the table and histogram back to zero
+        for (int i = tid; i < nu; i += kSumHashThreads) tab[uslot[i]] = 0u;
+        for (int i = tid; i < 256; i += kSumHashThreads) hist[i] = 0u;
+        __syncthreads();
+    }
+}
+
+// Larger blocks: the max + 1 of every term in a table of `dim` words (0: the
+// term is not in the block), the block's terms listed as first met.
+// Ties at the cut level are taken in term order by a scan of the table.
+template <bool kWrite>
+__global__ void __launch_bounds__(kSumDenseThreads) sum_u8_dense_kernel(SumU8Args a) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int dim = a.f.dim;
+    uint32_t* tab = reinterpret_cast<uint32_t*>(sm);
+    uint32_t* hist = tab + dim;
+    uint16_t* ulist = reinterpret_cast<uint16_t*>(hist + 256);
+    __shared__ unsigned s_nu, s_out, s_ntied;
+    __shared__ uint32_t s_mass;
+    __shared__ SumCut s_cut;
+    __shared__ unsigned wtot[kSumDenseThreads / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int kWarps = kSumDenseThreads / 32;
+    for (int i = tid; i < dim; i += kSumDenseThreads) tab[i] = 0u;
+    for (int i = tid; i < 256; i += kSumDenseThreads) hist[i] = 0u;
+    for (int64_t j = blockIdx.x; j < a.n_ids; j += gridDim.x) {
+        const int64_t b = a.ids[j];
+        if (tid == 0) {
+            s_nu = 0u;
+            s_out = 0u;
+            s_ntied = 0u;
+            s_mass = 0u;
+        }
+        __syncthreads();
+        const int64_t d0 = a.bdp[b], d1 = a.bdp[b + 1];
+        for (int64_t d = d0 + warp; d < d1; d += kWarps) {
+            const uint2 ri = __ldg(a.f.rowinfo + a.docs[d]);
+            const int64_t rb = static_cast<int64_t>(ri.x) * nsp::kRowAlign;
+            const int len = static_cast<int>(ri.y);
+            for (int e0 = 0; e0 < len; e0 += 256) {
+                const int e = e0 + 8 * lane;
+                uint32_t tw[4] = {0u, 0u, 0u, 0u};
+                uint2 cw = make_uint2(0u, 0u);
+                if (e < len) row8(a.f, rb, e, tw, cw);
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    bool first = false;
+                    uint32_t t = 0u;
+                    if (e + u < len) {
+                        t = term8(tw, u);
+                        first = atomicMax(&tab[t], code8(cw, u) + 1u) == 0u;
+                    }
+                    const int o = warp_append(&s_nu, first, lane);
+                    if (first) ulist[o] = static_cast<uint16_t>(t);
+                }
+            }
+        }
+        __syncthreads();
+        const int nu = static_cast<int>(s_nu);
+        uint32_t m = 0u;
+        for (int i = tid; i < nu; i += kSumDenseThreads) {
+            const uint32_t v = tab[ulist[i]] - 1u;
+            m += v;
+            atomicAdd(&hist[v], 1u);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m += __shfl_xor_sync(kFull, m, o);
+        if (lane == 0 && m > 0u) atomicAdd(&s_mass, m);
+        __syncthreads();
+        if (warp == 0) {
+            const SumCut c = sum_u8_cut(hist, s_mass, nu, a.alpha, lane);
+            if (lane == 0) s_cut = c;
+        }
+        __syncthreads();
+        const SumCut cut = s_cut;
+        if constexpr (!kWrite) {
+            if (tid == 0) a.keep[b] = cut.keep;
+        } else {
+            const uint32_t ntied = cut.vstar >= 0 ? hist[cut.vstar] : 0u;
+            const bool partial = cut.vstar >= 0 && static_cast<uint32_t>(cut.r) < ntied;
+            const int64_t out0 = a.kept_off[b - a.b0];
+            const uint32_t bl = a.block_local[b - a.b0];
+            // every pair above the cut level (all of that level when it is
+            // kept whole)
+            for (int base = 0; base < nu; base += kSumDenseThreads) {
+                const int i = base + tid;
+                uint32_t t = 0u;
+                int v = -1;
+                if (i < nu) {
+                    t = ulist[i];
+                    v = static_cast<int>(tab[t]) - 1;
+                }
+                const bool kept =
+                    i < nu && (cut.vstar < 0 || v > cut.vstar || (v == cut.vstar && !partial));
+                const int o = warp_append(&s_out, kept, lane);
+                if (kept) {
+                    a.tkey[out0 + o] = (t << 16) | bl;
+                    a.tval[out0 + o] = static_cast<float>(v);
+                }
+            }
+            if (partial) {
+                // the level's first r terms in term order: thread i scans
+                // terms [i * span, (i + 1) * span)
+                const int span = (dim + kSumDenseThreads - 1) / kSumDenseThreads;
+                const int lo = tid * span, hi = min(dim, lo + span);
+                const uint32_t want = static_cast<uint32_t>(cut.vstar) + 1u;
+                unsigned mine = 0u;
+                for (int t = lo; t < hi; ++t) mine += tab[t] == want ? 1u : 0u;
+                unsigned incl = mine;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const unsigned x = __shfl_up_sync(kFull, incl, o);
+                    if (lane >= o) incl += x;
+                }
+                if (lane == 31) wtot[warp] = incl;
+                __syncthreads();
+                unsigned before = incl - mine;
+                for (int w = 0; w < warp; ++w) before += wtot[w];
+                for (int t = lo; t < hi && before < static_cast<unsigned>(cut.r); ++t) {
+                    if (tab[t] != want) continue;
+                    const unsigned o = atomicAdd(&s_out, 1u);
+                    a.tkey[out0 + o] = (static_cast<uint32_t>(t) << 16) | bl;
+                    a.tval[out0 + o] = static_cast<float>(cut.vstar);
+                    ++before;
+                }
+            }
+        }
+        __syncthreads();
+        for (int i = tid; i < nu; i += kSumDenseThreads) tab[ulist[i]] = 0u;
+        for (int i = tid; i < 256; i += kSumDenseThreads) hist[i] = 0u;
+        __syncthreads();
+    }
+}
+
 struct SumPool {
     DevArray<int64_t> doc_eoff, flag, pos, first_run, pair_off, kept_off, rflag, rpos, o_start,
         o_lcol;
@@ -821,6 +1295,77 @@ struct SumPool {
     DevArray<uint8_t> has_delta, o_val, sort_tmp, tie;
     DevArray<uint64_t> pkey, pkey2;
 };
+
+// Kept summary pairs of the lists [t0, t1) -- tkey (term << 16 | block
+// within its list) and tval in P, list_koff[l] the first pair of list t0 + l
+// -- become the lists' summary columns, term-major per list
+// (build_transpose, inverted_list_clusters.cpp:230-293), appended to `out`.
+template <int ESZ>
+void emit_columns(nsp::SeismicHost& L, int32_t t0, int32_t t1,
+                  const std::vector<int64_t>& list_koff, int64_t n_kept, cudaStream_t s,
+                  SumPool& P, DevColumns& out) {
+    const int sms = nsp::device_sm_count();
+    const int64_t nk1 = std::max<int64_t>(n_kept, 1);
+    const std::vector<int32_t> list_koff32 = to_i32_offsets(list_koff);
+    P.list_koff.upload(list_koff32.data(), list_koff32.size(), s);
+    segmented_sort_pairs(P.tkey.data(), P.tkey2.data(), P.tval.data(), P.tval2.data(), n_kept,
+                         t1 - t0, P.list_koff.data(), s, /*stable=*/false, &P.sort_tmp);
+    g_steps.mark("transpose sort");
+    // columns assembled on the device: block ids, values, and one run per
+    // (list, term) with its start
+    const int32_t nl = t1 - t0;
+    P.o_blk.grow(nk1);
+    P.o_val.grow(nk1 * ESZ);
+    P.rflag.grow(n_kept + 1);
+    P.rpos.grow(n_kept + 1);
+    columns_kernel<ESZ><<<sms * 8, 256, 0, s>>>(P.tkey2.data(), P.tval2.data(), n_kept,
+                                                P.o_blk.data(), P.o_val.data(), P.rflag.data());
+    cuda_check(cudaGetLastError(), "columns_kernel");
+    list_start_kernel<<<std::max(1, (nl + 255) / 256), 256, 0, s>>>(P.list_koff.data(), nl,
+                                                                    n_kept, P.rflag.data());
+    cuda_check(cudaGetLastError(), "list_start_kernel");
+    nsp::exclusive_scan_i64(P.rflag.data(), P.rpos.data(), n_kept + 1, s);
+    int64_t n_cols = 0;
+    cuda_check(cudaMemcpyAsync(&n_cols, P.rpos.data() + n_kept, 8, cudaMemcpyDeviceToHost, s),
+               "D2H");
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    P.o_term.grow(std::max<int64_t>(n_cols, 1));
+    P.o_start.grow(std::max<int64_t>(n_cols, 1));
+    P.o_lcol.grow(static_cast<size_t>(nl) + 1);
+    column_compact_kernel<<<sms * 8, 256, 0, s>>>(P.tkey2.data(), P.rflag.data(), P.rpos.data(),
+                                                  n_kept, P.o_term.data(), P.o_start.data());
+    cuda_check(cudaGetLastError(), "column_compact_kernel");
+    list_cols_kernel<<<std::max(1, (nl + 1 + 255) / 256), 256, 0, s>>>(
+        P.list_koff.data(), nl, P.rpos.data(), P.o_lcol.data());
+    cuda_check(cudaGetLastError(), "list_cols_kernel");
+    // appended to the index's device columns; only the per-list column
+    // counts come back to the host
+    const size_t eb = out.n_entries, cb = out.n_cols;
+    dev_append(out.sblk, eb, P.o_blk.data(), static_cast<size_t>(n_kept), s);
+    dev_append(out.sval, eb * ESZ, P.o_val.data(), static_cast<size_t>(n_kept) * ESZ, s);
+    dev_append(out.sterm, cb, P.o_term.data(), static_cast<size_t>(n_cols), s);
+    if (out.srun.size() < cb + 1 + static_cast<size_t>(n_cols)) {
+        DevArray<int64_t> bigger(
+            std::max(out.srun.size() * 2, cb + 1 + static_cast<size_t>(n_cols)));
+        cuda_check(cudaMemcpyAsync(bigger.data(), out.srun.data(), (cb + 1) * sizeof(int64_t),
+                                   cudaMemcpyDeviceToDevice, s),
+                   "D2D");
+        cuda_check(cudaStreamSynchronize(s), "sync");
+        out.srun = std::move(bigger);
+    }
+    if (n_cols > 0)
+        column_bounds_kernel<<<sms * 4, 256, 0, s>>>(P.o_start.data(), n_cols,
+                                                     static_cast<int64_t>(eb), n_kept,
+                                                     out.srun.data() + cb + 1);
+    cuda_check(cudaGetLastError(), "column_bounds_kernel");
+    std::vector<int64_t> h_lcol(static_cast<size_t>(nl) + 1);
+    P.o_lcol.download(h_lcol.data(), h_lcol.size(), s);
+    cuda_check(cudaStreamSynchronize(s), "D2H");
+    out.n_entries += static_cast<size_t>(n_kept);
+    out.n_cols += static_cast<size_t>(n_cols);
+    for (int32_t l = 0; l < nl; ++l) L.ltp.push_back(static_cast<int64_t>(cb) + h_lcol[l + 1]);
+    g_steps.mark("columns");
+}
 
 template <int ESZ>
 void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
@@ -986,66 +1531,127 @@ void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
                                               P.tkey.data(), P.tval.data());
     cuda_check(cudaGetLastError(), "kept_pairs_kernel");
     g_steps.mark("alpha cut");
-    // term-major per list (build_transpose, inverted_list_clusters.cpp:230-293)
-    const std::vector<int32_t> list_koff32 = to_i32_offsets(list_koff);
-    P.list_koff.upload(list_koff32.data(), list_koff32.size(), s);
-    segmented_sort_pairs(P.tkey.data(), P.tkey2.data(), P.tval.data(), P.tval2.data(), n_kept,
-                         t1 - t0, P.list_koff.data(), s, /*stable=*/false, &P.sort_tmp);
-    g_steps.mark("transpose sort");
-    // columns assembled on the device: block ids, values, and one run per
-    // (list, term) with its start
-    const int32_t nl = t1 - t0;
-    P.o_blk.grow(nk1);
-    P.o_val.grow(nk1 * ESZ);
-    P.rflag.grow(n_kept + 1);
-    P.rpos.grow(n_kept + 1);
-    columns_kernel<ESZ><<<sms * 8, 256, 0, s>>>(P.tkey2.data(), P.tval2.data(), n_kept,
-                                                P.o_blk.data(), P.o_val.data(), P.rflag.data());
-    cuda_check(cudaGetLastError(), "columns_kernel");
-    list_start_kernel<<<std::max(1, (nl + 255) / 256), 256, 0, s>>>(P.list_koff.data(), nl,
-                                                                    n_kept, P.rflag.data());
-    cuda_check(cudaGetLastError(), "list_start_kernel");
-    nsp::exclusive_scan_i64(P.rflag.data(), P.rpos.data(), n_kept + 1, s);
-    int64_t n_cols = 0;
-    cuda_check(cudaMemcpyAsync(&n_cols, P.rpos.data() + n_kept, 8, cudaMemcpyDeviceToHost, s),
-               "D2H");
-    cuda_check(cudaStreamSynchronize(s), "sync");
-    P.o_term.grow(std::max<int64_t>(n_cols, 1));
-    P.o_start.grow(std::max<int64_t>(n_cols, 1));
-    P.o_lcol.grow(static_cast<size_t>(nl) + 1);
-    column_compact_kernel<<<sms * 8, 256, 0, s>>>(P.tkey2.data(), P.rflag.data(), P.rpos.data(),
-                                                  n_kept, P.o_term.data(), P.o_start.data());
-    cuda_check(cudaGetLastError(), "column_compact_kernel");
-    list_cols_kernel<<<std::max(1, (nl + 1 + 255) / 256), 256, 0, s>>>(
-        P.list_koff.data(), nl, P.rpos.data(), P.o_lcol.data());
-    cuda_check(cudaGetLastError(), "list_cols_kernel");
-    // appended to the index's device columns; only the per-list column
-    // counts come back to the host
-    const size_t eb = out.n_entries, cb = out.n_cols;
-    dev_append(out.sblk, eb, P.o_blk.data(), static_cast<size_t>(n_kept), s);
-    dev_append(out.sval, eb * ESZ, P.o_val.data(), static_cast<size_t>(n_kept) * ESZ, s);
-    dev_append(out.sterm, cb, P.o_term.data(), static_cast<size_t>(n_cols), s);
-    if (out.srun.size() < cb + 1 + static_cast<size_t>(n_cols)) {
-        DevArray<int64_t> bigger(
-            std::max(out.srun.size() * 2, cb + 1 + static_cast<size_t>(n_cols)));
-        cuda_check(cudaMemcpyAsync(bigger.data(), out.srun.data(), (cb + 1) * sizeof(int64_t),
-                                   cudaMemcpyDeviceToDevice, s),
-                   "D2D");
-        cuda_check(cudaStreamSynchronize(s), "sync");
-        out.srun = std::move(bigger);
+    emit_columns<ESZ>(L, t0, t1, list_koff, n_kept, s, P, out);
+}
+
+// Dynamic shared memory of the large-block kernel: a word and a list entry
+// per term, and the histogram.
+size_t sum_u8_dense_smem(int dim) {
+    return static_cast<size_t>(dim) * 4 + 256 * 4 + static_cast<size_t>(dim) * 2;
+}
+
+// Whether the fused uint8 summaries run on this device for this dimension.
+bool sum_u8_fits(int dim) {
+    int dev = 0, optin = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    cuda_check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev),
+               "cudaDeviceGetAttribute");
+    return sum_u8_dense_smem(dim) <= static_cast<size_t>(optin);
+}
+
+// Summaries of every block of a uint8 index (section 5' above): a count
+// pass over all blocks, then, per batch of lists bounded by kept pairs, a
+// write pass and the term-major columns.
+void summarize_u8(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
+                  const DevArray<int64_t>& d_bdp, nsp::SeismicHost& L,
+                  const std::vector<int64_t>& blk_e, float alpha, cudaStream_t s, SumPool& P,
+                  DevColumns& out) {
+    const int sms = nsp::device_sm_count();
+    const int64_t n_blocks = L.lbp.back();
+    const int32_t n_lists = L.n_lists();
+    std::vector<int64_t> small, big;
+    for (int64_t b = 0; b < n_blocks; ++b)
+        (blk_e[b + 1] - blk_e[b] <= kSumHashEntries ? small : big).push_back(b);
+    DevArray<int64_t> d_small, d_big;
+    if (!small.empty()) to_dev(d_small, small, s);
+    if (!big.empty()) to_dev(d_big, big, s);
+    const size_t dense_smem = sum_u8_dense_smem(f.dim);
+    cuda_check(cudaFuncSetAttribute(sum_u8_dense_kernel<false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(dense_smem)),
+               "cudaFuncSetAttribute");
+    cuda_check(cudaFuncSetAttribute(sum_u8_dense_kernel<true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(dense_smem)),
+               "cudaFuncSetAttribute");
+    auto launch = [&](SumU8Args a, int64_t s0, int64_t s1, int64_t g0, int64_t g1, bool write) {
+        if (s1 > s0) {
+            a.ids = d_small.data() + s0;
+            a.n_ids = s1 - s0;
+            const int grid = static_cast<int>(std::min<int64_t>(a.n_ids, int64_t{sms} * 8));
+            if (write)
+                sum_u8_hash_kernel<true><<<grid, kSumHashThreads, 0, s>>>(a);
+            else
+                sum_u8_hash_kernel<false><<<grid, kSumHashThreads, 0, s>>>(a);
+            cuda_check(cudaGetLastError(), "sum_u8_hash_kernel");
+        }
+        if (g1 > g0) {
+            a.ids = d_big.data() + g0;
+            a.n_ids = g1 - g0;
+            const int grid = static_cast<int>(std::min<int64_t>(a.n_ids, sms));
+            if (write)
+                sum_u8_dense_kernel<true><<<grid, kSumDenseThreads, dense_smem, s>>>(a);
+            else
+                sum_u8_dense_kernel<false><<<grid, kSumDenseThreads, dense_smem, s>>>(a);
+            cuda_check(cudaGetLastError(), "sum_u8_dense_kernel");
+        }
+    };
+    SumU8Args a{};
+    a.f = f;
+    a.docs = d_docs.data();
+    a.bdp = d_bdp.data();
+    a.alpha = alpha;
+    DevArray<int32_t> keep(static_cast<size_t>(std::max<int64_t>(n_blocks, 1)));
+    a.keep = keep.data();
+    launch(a, 0, static_cast<int64_t>(small.size()), 0, static_cast<int64_t>(big.size()), false);
+    const std::vector<int32_t> h_keep = to_host(keep, static_cast<size_t>(n_blocks), s);
+    std::vector<int64_t> kept_off(static_cast<size_t>(n_blocks) + 1, 0);
+    for (int64_t b = 0; b < n_blocks; ++b) kept_off[b + 1] = kept_off[b] + h_keep[b];
+    g_steps.mark("u8 count");
+    const int64_t budget = int64_t{1} << 27;  // kept pairs per batch
+    int32_t t0 = 0;
+    while (t0 < n_lists) {
+        int32_t t1 = t0 + 1;
+        while (t1 < n_lists && kept_off[L.lbp[t1 + 1]] - kept_off[L.lbp[t0]] <= budget) ++t1;
+        const int64_t b0 = L.lbp[t0], b1 = L.lbp[t1];
+        const int64_t nb = b1 - b0;
+        const int64_t n_kept = kept_off[b1] - kept_off[b0];
+        if (n_kept == 0) {
+            for (int32_t t = t0; t < t1; ++t) L.ltp.push_back(L.ltp.back());
+            t0 = t1;
+            continue;
+        }
+        std::vector<int64_t> rel(static_cast<size_t>(nb) + 1);
+        for (int64_t b = 0; b <= nb; ++b) rel[b] = kept_off[b0 + b] - kept_off[b0];
+        std::vector<uint16_t> block_local(static_cast<size_t>(nb));
+        std::vector<int64_t> list_koff(static_cast<size_t>(t1 - t0) + 1, 0);
+        for (int32_t t = t0; t < t1; ++t) {
+            for (int64_t b = L.lbp[t]; b < L.lbp[t + 1]; ++b)
+                block_local[b - b0] = static_cast<uint16_t>(b - L.lbp[t]);
+            list_koff[t - t0 + 1] = rel[L.lbp[t + 1] - b0];
+        }
+        P.kept_off.upload(rel.data(), rel.size(), s);
+        P.block_local.upload(block_local.data(), block_local.size(), s);
+        const size_t nk1 = static_cast<size_t>(std::max<int64_t>(n_kept, 1));
+        P.tkey.grow(nk1);
+        P.tkey2.grow(nk1);
+        P.tval.grow(nk1);
+        P.tval2.grow(nk1);
+        SumU8Args w = a;
+        w.kept_off = P.kept_off.data();
+        w.block_local = P.block_local.data();
+        w.b0 = b0;
+        w.tkey = P.tkey.data();
+        w.tval = P.tval.data();
+        const int64_t s0 = std::lower_bound(small.begin(), small.end(), b0) - small.begin();
+        const int64_t s1 = std::lower_bound(small.begin(), small.end(), b1) - small.begin();
+        const int64_t g0 = std::lower_bound(big.begin(), big.end(), b0) - big.begin();
+        const int64_t g1 = std::lower_bound(big.begin(), big.end(), b1) - big.begin();
+        launch(w, s0, s1, g0, g1, true);
+        g_steps.mark("u8 write");
+        emit_columns<1>(L, t0, t1, list_koff, n_kept, s, P, out);
+        t0 = t1;
     }
-    if (n_cols > 0)
-        column_bounds_kernel<<<sms * 4, 256, 0, s>>>(P.o_start.data(), n_cols,
-                                                     static_cast<int64_t>(eb), n_kept,
-                                                     out.srun.data() + cb + 1);
-    cuda_check(cudaGetLastError(), "column_bounds_kernel");
-    std::vector<int64_t> h_lcol(static_cast<size_t>(nl) + 1);
-    P.o_lcol.download(h_lcol.data(), h_lcol.size(), s);
-    cuda_check(cudaStreamSynchronize(s), "D2H");
-    out.n_entries += static_cast<size_t>(n_kept);
-    out.n_cols += static_cast<size_t>(n_cols);
-    for (int32_t l = 0; l < nl; ++l) L.ltp.push_back(static_cast<int64_t>(cb) + h_lcol[l + 1]);
-    g_steps.mark("columns");
 }
 
 // fp32 lists whose kept postings hold tied values get the reference's kept
@@ -1304,6 +1910,10 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
     cols.srun.resize(1);
     cuda_check(cudaMemsetAsync(cols.srun.data(), 0, sizeof(int64_t), s), "memset");
     int32_t t0 = 0;
+    if (ESZ == 1 && sum_u8_fits(dim)) {
+        summarize_u8(f, d_docs, d_bdp, L, blk_e, p.alpha, s, pool, cols);
+        t0 = n_lists;
+    }
     while (t0 < n_lists) {
         int32_t t1 = t0 + 1;
         while (t1 < n_lists && blk_e[L.lbp[t1 + 1]] - blk_e[L.lbp[t0]] <= budget) ++t1;
