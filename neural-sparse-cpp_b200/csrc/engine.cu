@@ -702,6 +702,7 @@ void run_seismic(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,
         a.cluster = p.cluster;
         a.seg_cap = p.seg_cap;
         a.sel_q = args.d_sel_q;
+        a.done = args.d_done;
         a.bscore = static_cast<float*>(ws.dev(
             Workspace::kBScore, static_cast<size_t>(p.blocks) * p.wpb * maxb * sizeof(float)));
         a.order_stride = (maxb + 7) & ~7;
@@ -903,6 +904,34 @@ void seismic_search(const ForwardDevice& fwd, const SeismicDevice& ix, const Que
     run_seismic(fwd, ix, q.n, u.indptr, u.idx, vals, q.max_nnz, args, d_sel, dd, dl, s, ws, stats);
     download_results(ws, q.n, args.k, dd, dl, out_d, out_l);
     check_kernel_error(ws, s);
+}
+
+void seismic_search_start(const ForwardDevice& fwd, const SeismicDevice& ix, const QueryBatch& q,
+                          const SeismicSearchArgs& args_in, float* out_d, int32_t* out_l,
+                          int32_t* done) {
+    SeismicSearchArgs args = args_in;
+    if (args.variant < 0) args.variant = kDefaultVariant;
+    if (args.plain || args.variant < 2 || done == nullptr)
+        throw std::invalid_argument("per-query completion needs a batched one-CTA-per-query "
+                                    "kernel variant and a flag per query");
+    args.d_done = done;
+    Workspace& ws = Workspace::get();
+    cudaStream_t s = ws.stream();
+    const Uploaded u = upload_queries(ws, q);
+    const void* vals = u.val;
+    if (args.qbits != 0) {
+        void* codes = ws.dev(Workspace::kQCode, static_cast<size_t>(u.nnz) * 2 + 16);
+        cuda_check(launch_sq_encode(u.val, codes, u.nnz, args.qbits, args.q_vmin, args.q_scale, s),
+                   "query encode");
+        vals = codes;
+    }
+    run_seismic(fwd, ix, q.n, u.indptr, u.idx, vals, q.max_nnz, args, nullptr, out_d, out_l, s,
+                ws, nullptr);
+}
+
+void seismic_search_wait() {
+    Workspace& ws = Workspace::get();
+    check_kernel_error(ws, ws.stream());
 }
 
 void seismic_search_device(const ForwardDevice& fwd, const SeismicDevice& ix, int32_t n,

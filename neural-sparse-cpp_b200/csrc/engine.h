@@ -296,6 +296,9 @@ struct SeismicSearchArgs {
     // doc per CTA, on a grid of one CTA per SM)
     bool count_unique = false;
     int32_t nnz_cap = -1;     // entries the query arrays hold (negative: not checked)
+    // variants 2-5: per query, set to 1 once its results are written (see
+    // seismic_search_start), or nullptr
+    int32_t* d_done = nullptr;
 };
 
 // Device scratch a batched (not plain) run_seismic of `n` queries with `args`
@@ -309,6 +312,17 @@ struct SeismicScratchNeed {
 };
 SeismicScratchNeed seismic_scratch_need(const ForwardDevice& fwd, const SeismicDevice& ix,
                                         int32_t n, int32_t max_nnz, const SeismicSearchArgs& args);
+
+// Host queries in; results written by the kernel straight to `out_d` /
+// `out_l` (addresses the device can write and the host can read: mapped
+// pinned memory), done[i] set to 1 after query i's -- so a caller can take
+// each query's results as it finishes. Returns once the launch is queued on
+// this thread's stream; seismic_search_wait() then waits for it and raises
+// the kernel's errors. Batched one-CTA-per-query kernels only.
+void seismic_search_start(const ForwardDevice& fwd, const SeismicDevice& ix, const QueryBatch& q,
+                          const SeismicSearchArgs& args, float* out_d, int32_t* out_l,
+                          int32_t* done);
+void seismic_search_wait();
 
 // Host buffers in, host buffers out (the reference-facing path).
 void seismic_search(const ForwardDevice& fwd, const SeismicDevice& ix, const QueryBatch& q,

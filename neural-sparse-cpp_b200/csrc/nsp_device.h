@@ -119,6 +119,9 @@ struct SeismicLaunch {
     int32_t stage_bytes;
     int32_t bcap;
     int32_t* err;               // nonzero: a kernel-side error (see check_kernel_error)
+    // variants 2-5, or nullptr: done[q] is set to 1 once query q's results are
+    // written (system scope: the host may read both from mapped memory)
+    int32_t* done;
     // Variants 2-5 (one CTA per query): candidate docs per batch, lanes per
     // scored doc (1, 2, 4, 8), and per-CTA scratch -- `bscore` holds warps *
     // max_blocks floats per CTA, `order` the first list's visiting order,

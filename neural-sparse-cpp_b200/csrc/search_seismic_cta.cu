@@ -1088,9 +1088,17 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
         }
         // results, padded with (-1.0, -1); SQ scores decoded
         // (seismic_scalar_quantized_index.cpp:345-355)
-        if (warp == 0)
+        if (warp == 0) {
             heap_emit(hs, hid, n, a.k, a.decode_scale, a.out_d + static_cast<size_t>(q) * a.k,
                       a.out_l + static_cast<size_t>(q) * a.k, lane);
+            if (a.done != nullptr) {
+                // every lane's results reach memory (mapped host memory
+                // included) before the flag does
+                __threadfence_system();
+                __syncwarp();
+                if (lane == 0) *reinterpret_cast<volatile int32_t*>(a.done + q) = 1;
+            }
+        }
         if (a.stats != nullptr) {
             // per warp: its threads' doc counts and row bytes, plus its
             // summary bytes (the same on every lane) and, for warp 0, the

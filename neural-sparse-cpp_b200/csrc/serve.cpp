@@ -10,10 +10,14 @@
 // requests that arrive meanwhile are taken by the next free worker, so
 // batches overlap on the GPU (continuous batching, no fixed batching window).
 // Each request's result is exactly what a search of that query alone returns:
-// the kernel treats every query on its own, with its own heap.
+// the kernel treats every query on its own, with its own heap. A request
+// completes as soon as its own query's results are written: the kernel
+// writes them, with a done flag per query, into the worker's mapped host
+// memory, and the worker polls the flags while the launch runs.
 #include "serve.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <stdexcept>
 #include <thread>
@@ -33,6 +37,37 @@ using Clock = std::chrono::steady_clock;
 // their batches grow the scratch once).
 constexpr int kReserveK = 100;
 constexpr int kReserveNnz = 256;
+
+// Page-locked host memory the device writes into (cudaHostAllocMapped): a
+// worker's results and per-query done flags, read by the host while the
+// launch still runs.
+template <class T>
+struct Mapped {
+    T* h = nullptr;  // host address
+    T* d = nullptr;  // the device's address of the same memory
+    size_t n = 0;
+    Mapped() = default;
+    Mapped(const Mapped&) = delete;
+    Mapped& operator=(const Mapped&) = delete;
+    ~Mapped() {
+        if (h != nullptr) cudaFreeHost(h);
+    }
+    // Room for `want` elements; only between launches (the old memory goes).
+    void grow(size_t want) {
+        if (want <= n) return;
+        if (h != nullptr) cudaFreeHost(h);
+        h = nullptr;
+        d = nullptr;
+        n = 0;
+        void* p = nullptr;
+        nsp::cuda_check(cudaHostAlloc(&p, want * sizeof(T), cudaHostAllocMapped), "cudaHostAlloc");
+        h = static_cast<T*>(p);
+        void* dp = nullptr;
+        nsp::cuda_check(cudaHostGetDevicePointer(&dp, p, 0), "cudaHostGetDevicePointer");
+        d = static_cast<T*>(dp);
+        n = want;
+    }
+};
 
 int64_t request_bytes(const ServerRequest& r) {
     // query terms and values, results, one selector pointer
@@ -218,7 +253,15 @@ ServerStats Server::stats() const {
 void Server::worker() {
     if (cudaSetDevice(device_) != cudaSuccess) return;
     nsp::DevArray<const uint64_t*> d_sel;  // this worker's per-query selector table
+    // the kernel writes each query's results and its done flag here, so a
+    // request completes when its own query does, not when the launch's
+    // slowest query does
+    Mapped<float> md;
+    Mapped<int32_t> ml, mdone;
     try {
+        md.grow(static_cast<size_t>(cfg_.max_batch) * kReserveK);
+        ml.grow(static_cast<size_t>(cfg_.max_batch) * kReserveK);
+        mdone.grow(static_cast<size_t>(cfg_.max_batch));
         // Scratch for every batch size up to max_batch (rows up to kReserveNnz
         // terms, k up to kReserveK) before the first request: a buffer grown
         // mid-stream frees the old one, and that cudaFree waits for every
@@ -285,8 +328,29 @@ void Server::worker() {
         std::string error;
         const int n = static_cast<int>(batch.size());
         const int k = batch[0]->k;
-        std::vector<float> d(static_cast<size_t>(n) * k);
-        std::vector<int32_t> l(static_cast<size_t>(n) * k);
+        std::vector<char> fin(static_cast<size_t>(n), 0);
+        int left = n;
+        // requests whose results are in the mapped buffers: done, under the lock
+        auto complete = [&](const std::vector<int>& ready) {
+            std::lock_guard<std::mutex> g(mu_);
+            const Clock::time_point now = Clock::now();
+            for (const int i : ready) {
+                ServerRequest& r = *batch[i];
+                r.d.assign(md.h + static_cast<size_t>(i) * k, md.h + static_cast<size_t>(i + 1) * k);
+                r.l.resize(static_cast<size_t>(k));
+                for (int j = 0; j < k; ++j) {
+                    const int32_t v = ml.h[static_cast<size_t>(i) * k + j];
+                    int64_t out = v;
+                    if (v >= 0 && !ext_ids_.empty())
+                        out = ext_ids_[v];
+                    else if (v >= 0 && id_map_ != nullptr)
+                        out = (*id_map_)[v];
+                    r.l[j] = out;
+                }
+                r.t_done = now;
+                r.done = true;
+            }
+        };
         try {
             nsp::QueryBatch q;
             q.n = n;
@@ -318,8 +382,35 @@ void Server::worker() {
                 d_sel.upload(sel.data(), sel.size(), nsp::Workspace::get().stream());
                 a.d_sel_q = d_sel.data();
             }
-            nsp::seismic_search(st_->vectors.dev, st_->lists_dev, q, a, nullptr, d.data(),
-                                l.data(), nullptr);
+            md.grow(static_cast<size_t>(n) * k);
+            ml.grow(static_cast<size_t>(n) * k);
+            mdone.grow(static_cast<size_t>(n));
+            std::memset(mdone.h, 0, static_cast<size_t>(n) * sizeof(int32_t));
+            nsp::seismic_search_start(st_->vectors.dev, st_->lists_dev, q, a, md.d, ml.d,
+                                      mdone.d);
+            // each request completes when its query's flag is up; once the
+            // launch has ended, one more sweep finds the last flags
+            const cudaStream_t s = nsp::Workspace::get().stream();
+            const volatile int32_t* flags = mdone.h;
+            std::vector<int> ready;
+            bool ended = false;
+            for (;;) {
+                ready.clear();
+                for (int i = 0; i < n; ++i)
+                    if (!fin[i] && flags[i] != 0) ready.push_back(i);
+                if (!ready.empty()) {
+                    std::atomic_thread_fence(std::memory_order_acquire);
+                    complete(ready);
+                    cv_done_.notify_all();
+                    for (const int i : ready) fin[i] = 1;
+                    left -= static_cast<int>(ready.size());
+                }
+                if (left == 0 || ended) break;
+                ended = cudaStreamQuery(s) != cudaErrorNotReady;
+                if (!ended) std::this_thread::yield();
+            }
+            nsp::seismic_search_wait();  // raises the launch's errors
+            if (left > 0) throw std::runtime_error("a search launch ended without some results");
         } catch (const std::exception& e) {
             error = e.what();
         }
@@ -327,20 +418,11 @@ void Server::worker() {
             std::lock_guard<std::mutex> g(mu_);
             const Clock::time_point now = Clock::now();
             for (int i = 0; i < n; ++i) {
+                if (fin[i]) continue;
                 ServerRequest& r = *batch[i];
                 r.error = error;
-                r.d.assign(d.begin() + static_cast<size_t>(i) * k,
-                           d.begin() + static_cast<size_t>(i + 1) * k);
-                r.l.resize(static_cast<size_t>(k));
-                for (int j = 0; j < k; ++j) {
-                    const int32_t v = l[static_cast<size_t>(i) * k + j];
-                    int64_t out = v;
-                    if (v >= 0 && !ext_ids_.empty())
-                        out = ext_ids_[v];
-                    else if (v >= 0 && id_map_ != nullptr)
-                        out = (*id_map_)[v];
-                    r.l[j] = out;
-                }
+                r.d.assign(static_cast<size_t>(k), -1.0f);
+                r.l.assign(static_cast<size_t>(k), -1);
                 r.t_done = now;
                 r.done = true;
             }
