@@ -1534,6 +1534,28 @@ void summarize_batch(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
     emit_columns<ESZ>(L, t0, t1, list_koff, n_kept, s, P, out);
 }
 
+// Entries of each block (its docs' row lengths summed), for the choice
+// between the two kernels.
+__global__ void block_entries_kernel(nsp::FwdView f, const int32_t* docs, const int64_t* bdp,
+                                     int64_t nb, int32_t* ent) {
+    for (int64_t b = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; b < nb;
+         b += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        int64_t e = 0;
+        for (int64_t j = bdp[b]; j < bdp[b + 1]; ++j) e += f.rowinfo[docs[j]].y;
+        ent[b] = static_cast<int32_t>(e < INT32_MAX ? e : INT32_MAX);
+    }
+}
+
+std::vector<int32_t> block_entries(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
+                                   const DevArray<int64_t>& d_bdp, int64_t nb, cudaStream_t s) {
+    if (nb == 0) return {};
+    DevArray<int32_t> ent(static_cast<size_t>(nb));
+    const int sms = nsp::device_sm_count();
+    block_entries_kernel<<<sms * 8, 256, 0, s>>>(f, d_docs.data(), d_bdp.data(), nb, ent.data());
+    cuda_check(cudaGetLastError(), "block_entries_kernel");
+    return to_host(ent, static_cast<size_t>(nb), s);
+}
+
 // Dynamic shared memory of the large-block kernel: a word and a list entry
 // per term, and the histogram.
 size_t sum_u8_dense_smem(int dim) {
@@ -1554,14 +1576,14 @@ bool sum_u8_fits(int dim) {
 // write pass and the term-major columns.
 void summarize_u8(const nsp::FwdView& f, const DevArray<int32_t>& d_docs,
                   const DevArray<int64_t>& d_bdp, nsp::SeismicHost& L,
-                  const std::vector<int64_t>& blk_e, float alpha, cudaStream_t s, SumPool& P,
+                  const std::vector<int32_t>& blk_n, float alpha, cudaStream_t s, SumPool& P,
                   DevColumns& out) {
     const int sms = nsp::device_sm_count();
     const int64_t n_blocks = L.lbp.back();
     const int32_t n_lists = L.n_lists();
     std::vector<int64_t> small, big;
     for (int64_t b = 0; b < n_blocks; ++b)
-        (blk_e[b + 1] - blk_e[b] <= kSumHashEntries ? small : big).push_back(b);
+        (blk_n[b] <= kSumHashEntries ? small : big).push_back(b);
     DevArray<int64_t> d_small, d_big;
     if (!small.empty()) to_dev(d_small, small, s);
     if (!big.empty()) to_dev(d_big, big, s);
@@ -1885,19 +1907,25 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
 
     clock.mark("blocks");
     // ---- 5. summaries, in batches of lists bounded by entry count
-    std::vector<int64_t> doc_len(static_cast<size_t>(total_kept));
-    for (int64_t j = 0; j < total_kept; ++j) {
-        const int32_t d = L.docs[j];
-        doc_len[j] = h.indptr[d + 1] - h.indptr[d];
-    }
-    std::vector<int64_t> doc_eoff(static_cast<size_t>(total_kept) + 1, 0);
-    for (int64_t j = 0; j < total_kept; ++j) doc_eoff[j + 1] = doc_eoff[j] + doc_len[j];
-    std::vector<int64_t> blk_e(static_cast<size_t>(n_blocks) + 1, 0);
-    for (int64_t b = 0; b <= n_blocks; ++b) blk_e[b] = doc_eoff[L.bdp[b]];
+    const bool fused_u8 = ESZ == 1 && sum_u8_fits(dim);
     DevArray<int64_t> d_bdp;
     to_dev(d_bdp, L.bdp, s);
-    DevArray<int32_t> d_docs;
-    to_dev(d_docs, L.docs, s);
+    DevArray<int32_t> d_docs = std::move(bdocs);  // the block-ordered docs, still resident
+    std::vector<int64_t> doc_eoff, blk_e;
+    std::vector<int32_t> blk_n;  // fused uint8 path: entries per block
+    if (fused_u8) {
+        blk_n = block_entries(f, d_docs, d_bdp, n_blocks, s);
+    } else {
+        std::vector<int64_t> doc_len(static_cast<size_t>(total_kept));
+        for (int64_t j = 0; j < total_kept; ++j) {
+            const int32_t d = L.docs[j];
+            doc_len[j] = h.indptr[d + 1] - h.indptr[d];
+        }
+        doc_eoff.assign(static_cast<size_t>(total_kept) + 1, 0);
+        for (int64_t j = 0; j < total_kept; ++j) doc_eoff[j + 1] = doc_eoff[j] + doc_len[j];
+        blk_e.assign(static_cast<size_t>(n_blocks) + 1, 0);
+        for (int64_t b = 0; b <= n_blocks; ++b) blk_e[b] = doc_eoff[L.bdp[b]];
+    }
     const int64_t budget = int64_t{1} << 27;  // entries per batch
     g_steps.start(s);
     SumPool pool;
@@ -1910,8 +1938,8 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
     cols.srun.resize(1);
     cuda_check(cudaMemsetAsync(cols.srun.data(), 0, sizeof(int64_t), s), "memset");
     int32_t t0 = 0;
-    if (ESZ == 1 && sum_u8_fits(dim)) {
-        summarize_u8(f, d_docs, d_bdp, L, blk_e, p.alpha, s, pool, cols);
+    if (fused_u8) {
+        summarize_u8(f, d_docs, d_bdp, L, blk_n, p.alpha, s, pool, cols);
         t0 = n_lists;
     }
     while (t0 < n_lists) {
