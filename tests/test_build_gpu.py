@@ -191,6 +191,54 @@ def test_sq_build_assignment_and_summaries_match_reference(tmp_path):
     assert checked > 50
 
 
+@pytest.mark.parametrize("lam,beta,alpha", [(400, 2, 0.4), (400, 40, 0.1), (400, 40, 1.0),
+                                             (400, 2, 1.5), (60, 1, 0.7)])
+def test_sq_summaries_match_reference_on_large_blocks_and_edge_alphas(tmp_path, lam, beta,
+                                                                        alpha):
+    """uint8 summaries are made per block in shared memory, by a hash-table
+    kernel (blocks of up to 3,072 entries) or a per-term-table kernel (larger
+    blocks: beta 1-2 puts 60-200 docs in a block). For every list, the
+    reference's summarizer over the engine's blocks gives each block the
+    engine's entry count and values, at an alpha that keeps little (0.1),
+    one that ends at the last nonzero maximum (1.0) and one no running sum
+    reaches (1.5: every pair kept)."""
+    docs = synth.docs_config0(6000, seed=9)
+    vmin, vmax = float(docs.values.min()), float(docs.values.max())
+    spec = (f"seismic_sq,quantizer=8bit|vmin={vmin!r}|vmax={vmax!r}|lambda={lam}|beta={beta}|"
+            f"alpha={alpha}|seed=7")
+    device_build(docs, spec, tmp_path / "q.idx")
+    f = O.read_index_file(str(tmp_path / "q.idx"))
+    codes = O.sq_encode_u8(vmin, vmax, docs.values)
+    L = O.ref_lib("generic")
+    P = lambda a: a.ctypes.data  # noqa: E731
+    lens = np.diff(docs.indptr)
+    lists = [c for c in f["lists"] if len(c["offsets"]) >= 2]
+    largest = [c for c in lists if lens[c["docs"]].sum() > 3072]  # lists with a large block
+    rng = np.random.default_rng(2)
+    sample = [lists[i] for i in rng.choice(len(lists), min(150, len(lists)), replace=False)]
+    big = 0
+    checked = 0
+    cap = 1 << 24
+    buf = np.empty(cap, np.uint8)
+    for c in largest[:150] + sample:
+        off = c["offsets"]
+        n = L.ref_summarize(docs.dim, 1, docs.n, P(docs.indptr), P(docs.indices), P(codes),
+                            P(c["docs"]), P(off), len(off) - 1, alpha, P(buf), cap)
+        assert n > 0
+        r = O._read_clusters(O._Rd(bytes(buf[:n])))
+        nb = len(off) - 1
+        np.testing.assert_array_equal(np.bincount(c["csc_cluster"], minlength=nb),
+                                      np.bincount(r["csc_cluster"], minlength=nb))
+        for b in range(nb):
+            np.testing.assert_array_equal(np.sort(c["csc_value"][c["csc_cluster"] == b]),
+                                          np.sort(r["csc_value"][r["csc_cluster"] == b]))
+            big += int(lens[c["docs"][off[b]:off[b + 1]]].sum() > 3072)
+        checked += 1
+    assert checked > 100
+    if beta <= 2:
+        assert big > 0  # the per-term-table kernel ran
+
+
 def test_sq_build_full_size_lists_match_reference_assigner(tmp_path):
     """The 8.8M-doc build's list shape at 1M docs: postings capped at 6,000 and
     600 blocks per full list (uint8 codes, config-2 generator). For the 12
