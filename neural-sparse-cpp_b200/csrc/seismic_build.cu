@@ -251,7 +251,7 @@ __device__ __forceinline__ void add_product(assign_acc_t<ESZ>* sims, int32_t c,
 }
 
 template <int ESZ>
-__global__ void __launch_bounds__(256) assign_kernel(AssignArgs a) {
+__global__ void __launch_bounds__(1024) assign_kernel(AssignArgs a) {
     using acc_t = assign_acc_t<ESZ>;
     // centroid entries of one term in flight per lane: a term's run is
     // loaded kChunks * 32 entries at a time, the next hit term's first
@@ -1823,20 +1823,21 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
         for (int64_t d = 0; d < n_docs; ++d)
             max_row = std::max<int64_t>(max_row, h.indptr[d + 1] - h.indptr[d]);
         const int64_t max_ce = std::max<int64_t>(1, static_cast<int64_t>(max_nc) * max_row);
-        const int wpb = 8;
+        const int wpb = 32;
         const size_t acc_bytes = sizeof(assign_acc_t<ESZ>);
         const size_t sims_smem = static_cast<size_t>(wpb) * std::max(max_nc, 1) * acc_bytes;
-        const bool sims_in_smem = sims_smem <= 96u * 1024u;
+        const bool sims_in_smem = sims_smem <= 160u * 1024u;
         const size_t smem = sims_in_smem ? sims_smem : 0;
         if (sims_in_smem) cuda_check(nsp::allow_opt_in_smem(assign_kernel<ESZ>), "assign smem");
-        // as many resident CTAs as fit, up to 4 per SM (each list's
-        // similarity rows are walked with its memory round trips exposed,
-        // so resident warps are what hides them)
+        // one CTA of 32 warps per SM: as many warps as four CTAs of 8 hide
+        // the memory round trips with, and a quarter of the per-CTA term
+        // tables (trun, tcnt, ...), which then stay in L2 (8.8M SQ docs:
+        // 6.4 -> 5.5 s against four CTAs of 8 warps; two of 16: 5.7 s)
         int per_sm = 0;
         cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, assign_kernel<ESZ>,
                                                                  wpb * 32, smem),
                    "assign occupancy");
-        const int ctas = sms * std::max(1, std::min(per_sm, 4));
+        const int ctas = sms * std::max(1, std::min(per_sm, 1));
         DevArray<int32_t> tcnt(static_cast<size_t>(ctas) * dim), tstart(static_cast<size_t>(ctas) * dim),
             tcur(static_cast<size_t>(ctas) * dim), touched(static_cast<size_t>(ctas) * max_ce);
         DevArray<int2> trun(static_cast<size_t>(ctas) * dim);
