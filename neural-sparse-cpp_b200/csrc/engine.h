@@ -94,7 +94,8 @@ class Workspace : public Scratch {
 public:
     enum Slot : int {
         kQIndptr, kQIdx, kQVal, kQCode, kOutD, kOutL, kSel, kBScore, kCounter, kStats,
-        kCandD, kCandL, kHeapD, kHeapL, kQValG, kIds, kErr, kOrder, kSortKeys, kVisit, kNumSlots
+        kCandD, kCandL, kHeapD, kHeapL, kQValG, kIds, kErr, kOrder, kSortKeys, kVisit, kQOrder,
+        kNumSlots
     };
     static Workspace& get();
     cudaStream_t stream() const { return stream_; }

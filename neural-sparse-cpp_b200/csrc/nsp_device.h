@@ -119,6 +119,10 @@ struct SeismicLaunch {
     int32_t stage_bytes;
     int32_t bcap;
     int32_t* err;               // nonzero: a kernel-side error (see check_kernel_error)
+    // variants 2-5, batched, or nullptr: the order queries are claimed in
+    // (longest rows first, so the launch does not end on a long query
+    // claimed last); results do not depend on it
+    const int32_t* qorder;
     // variants 2-5, or nullptr: done[q] is set to 1 once query q's results are
     // written (system scope: the host may read both from mapped memory)
     int32_t* done;
@@ -236,6 +240,11 @@ cudaError_t launch_exact_list(int val_kind, const FwdView& fwd, const QueryView&
                               const int32_t* ids, int n_ids, int k, float decode_scale,
                               int32_t qcap, float* out_d, int32_t* out_l,
                               cudaStream_t s);
+
+// The claim order of a batched launch's queries: row lengths descending
+// (one CTA; any order among equal lengths).
+cudaError_t launch_order_by_length(const int32_t* indptr, int32_t n, int32_t* order,
+                                   cudaStream_t s);
 
 // ScalarQuantizer::encode (utils/scalar_quantizer.h:97-118) on the device.
 cudaError_t launch_sq_encode(const float* vals, void* codes, int64_t n, int qbits,

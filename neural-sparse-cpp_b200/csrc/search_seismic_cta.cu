@@ -746,9 +746,10 @@ __global__ void __launch_bounds__(1024, 1) seismic_cta_kernel(SeismicLaunch a) {
     for (;;) {
         if (tid == 0) {
             int q;
-            if (a.work_counter != nullptr)
+            if (a.work_counter != nullptr) {
                 q = atomicAdd(a.work_counter, 1);
-            else
+                if (a.qorder != nullptr && q < a.q.n) q = a.qorder[q];
+            } else
                 q = a.first_query + static_cast<int>(cid) + iter * static_cast<int>(ncl);
             ctl->q = q;
             ctl->nheap = 0;  // the query's heap starts empty
@@ -1225,6 +1226,31 @@ cudaError_t launch_cta_typed(const SeismicLaunch& a, int warps, int blocks, cuda
 
 // Table entries: fp32 queries hold ranks, one byte while the query has at
 // most 255 terms; SQ queries hold their codes.
+// Claim order of a batched launch: queries by row length, longest first (a
+// counting sort over lengths clamped to 255, one CTA).
+__global__ void __launch_bounds__(1024) order_by_length_kernel(const int32_t* indptr, int32_t n,
+                                                               int32_t* order) {
+    __shared__ int32_t bin[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) bin[i] = 0;
+    __syncthreads();
+    auto key = [&](int32_t i) {
+        const int32_t len = indptr[i + 1] - indptr[i];
+        return 255 - (len < 0 ? 0 : (len > 255 ? 255 : len));
+    };
+    for (int32_t i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&bin[key(i)], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int32_t run = 0;
+        for (int b = 0; b < 256; ++b) {
+            const int32_t c = bin[b];
+            bin[b] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    for (int32_t i = threadIdx.x; i < n; i += blockDim.x) order[atomicAdd(&bin[key(i)], 1)] = i;
+}
+
 static bool wide_table(int val_kind, int qcap) {
     return val_kind == kU16 || (val_kind == kF32 && qcap > 255);
 }
@@ -1257,6 +1283,13 @@ cudaError_t launch_seismic_cta(int val_kind, const SeismicLaunch& a, int warps, 
                                             : launch_cta_typed<float, uint8_t>(a, warps, blocks, s);
     if (val_kind == kU8) return launch_cta_typed<uint8_t, uint8_t>(a, warps, blocks, s);
     return launch_cta_typed<uint16_t, uint16_t>(a, warps, blocks, s);
+}
+
+cudaError_t launch_order_by_length(const int32_t* indptr, int32_t n, int32_t* order,
+                                   cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    order_by_length_kernel<<<1, 1024, 0, s>>>(indptr, n, order);
+    return cudaGetLastError();
 }
 
 }  // namespace nsp
