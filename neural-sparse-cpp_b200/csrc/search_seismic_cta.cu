@@ -229,7 +229,9 @@ __device__ __forceinline__ int partial_steps(const uint16_t* ip, const uint8_t* 
             v[s] = __ldg(reinterpret_cast<const uint4*>(vp + s * stride));
         }
     }
-    int acc = 0;
+    // four independent sums (integer: exact in any order), so the products
+    // do not wait on one another
+    int acc[4] = {0, 0, 0, 0};
 #pragma unroll
     for (int s = 0; s < kSteps; ++s) {
         if (s == 0 || rem > s * stride) {
@@ -237,11 +239,13 @@ __device__ __forceinline__ int partial_steps(const uint16_t* ip, const uint8_t* 
 #pragma unroll
             for (int u = 0; u < 16; ++u) {
                 const int q = static_cast<int>(tbl[term_of(t[s], u)]);
-                acc += static_cast<int>((w[u >> 2] >> (8 * (u & 3))) & 0xffu) * q;
+                // code byte u & 3 of its word, zero-extended (one byte permute)
+                const uint32_t x = __byte_perm(w[u >> 2], 0u, 0x4440u | (u & 3));
+                acc[u & 3] += static_cast<int>(x) * q;
             }
         }
     }
-    return acc;
+    return (acc[0] + acc[1]) + (acc[2] + acc[3]);
 }
 
 // uint16 codes: int64 sum (distance.h:49-57).
