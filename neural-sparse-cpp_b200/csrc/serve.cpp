@@ -413,6 +413,9 @@ void Server::worker() {
             if (left > 0) throw std::runtime_error("a search launch ended without some results");
         } catch (const std::exception& e) {
             error = e.what();
+            // nothing of this batch may still run when the mapped buffers
+            // are reused (or regrown) for the next one
+            cudaStreamSynchronize(nsp::Workspace::get().stream());
         }
         {
             std::lock_guard<std::mutex> g(mu_);
