@@ -727,7 +727,7 @@ nsp::KernelChoice seismic_autotune(Index* index, idx_t n, const idx_t* indptr,
     std::vector<idx_t> l(static_cast<size_t>(n) * k);
     nsp::KernelChoice best;
     for (int variant = 2; variant <= 5; ++variant) {
-        for (int batch : {256, 512, 1024}) {
+        for (int batch : {256, 512, 640, 1024}) {
             for (int warps : {4, 8}) {
                 nsp::SeismicSearchArgs t = a;
                 t.variant = variant;
