@@ -14,6 +14,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "engine.h"
@@ -476,19 +477,33 @@ float ScalarQuantizer::encode_scale() const {
     return kmax / (vmax_ - vmin_);
 }
 
-// scalar_quantizer.h:97-101 (8-bit) and 108-112 (16-bit).
+// scalar_quantizer.h:97-101 (8-bit) and 108-112 (16-bit). Each value is
+// encoded on its own, so large inputs are split over host threads (a corpus
+// of 1.24B values took seconds on one).
 void ScalarQuantizer::encode(const float* vals, uint8_t* codes, size_t n) const {
     const float kmax = qtype_ == QuantizerType::QT_8bit ? 255.0F : 65535.0F;
     const float scale = encode_scale();
-    for (size_t i = 0; i < n; ++i) {
-        float scaled = (vals[i] - vmin_) * scale;
-        scaled = std::max(0.0F, std::min(kmax, scaled));
-        const long r = std::lround(scaled);
-        if (qtype_ == QuantizerType::QT_8bit)
-            codes[i] = static_cast<uint8_t>(r);
-        else
-            reinterpret_cast<uint16_t*>(codes)[i] = static_cast<uint16_t>(r);
-    }
+    auto range = [&](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; ++i) {
+            float scaled = (vals[i] - vmin_) * scale;
+            scaled = std::max(0.0F, std::min(kmax, scaled));
+            const long r = std::lround(scaled);
+            if (qtype_ == QuantizerType::QT_8bit)
+                codes[i] = static_cast<uint8_t>(r);
+            else
+                reinterpret_cast<uint16_t*>(codes)[i] = static_cast<uint16_t>(r);
+        }
+    };
+    constexpr size_t kPerThread = size_t{1} << 22;
+    const size_t hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const size_t nth = std::min(hw, (n + kPerThread - 1) / kPerThread);
+    if (nth <= 1) return range(0, n);
+    std::vector<std::thread> pool;
+    const size_t step = (n + nth - 1) / nth;
+    for (size_t t = 1; t < nth; ++t)
+        pool.emplace_back(range, std::min(n, t * step), std::min(n, (t + 1) * step));
+    range(0, std::min(n, step));
+    for (auto& th : pool) th.join();
 }
 
 void ScalarQuantizer::decode(const uint8_t* codes, float* vals, size_t n) const {

@@ -1976,8 +1976,7 @@ void build_typed(SeismicState& st, int dim, const SeismicClusterParameters& p) {
 }  // namespace
 
 void seismic_build(SeismicState& st, int dim, const SeismicClusterParameters& params) {
-    for (uint16_t t : st.vectors.host.indices)
-        if (t >= dim) throw std::invalid_argument("term_id out of range");
+    if (!st.vectors.terms_in_range(dim)) throw std::invalid_argument("term_id out of range");
     const int esz = st.vectors.host.esz;
     if (st.vectors.host.n() == 0) {
         // no documents: one empty list per term

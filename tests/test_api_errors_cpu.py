@@ -82,3 +82,19 @@ def test_api_errors_match_reference(spec, tmp_path):
         finally:
             L.ref_index_free(h)
         assert ours == ref, name
+
+
+@pytest.mark.parametrize("spec", ["seismic,lambda=10|beta=2|alpha=0.4|seed=1",
+                                  "seismic_sq,quantizer=8bit|vmin=0.0|vmax=2.0|lambda=10|beta=2|"
+                                  "alpha=0.4|seed=1"])
+def test_seismic_build_rejects_out_of_range_terms_before_the_device(spec):
+    """build() checks every stored term against the dimension first (one scan,
+    kept for later calls), so a bad corpus fails with the reference's
+    exception and no device is needed to find out."""
+    idx = nsparse.index_factory(10, spec)
+    idx.add(2, np.array([0, 2, 3], np.int32), np.array([1, 20, 3], np.uint16),
+            np.ones(3, np.float32))
+    with pytest.raises(ValueError, match="term_id out of range"):
+        idx.build()
+    with pytest.raises(ValueError, match="term_id out of range"):
+        idx.build()
