@@ -159,6 +159,16 @@ def counting_pass(nsparse, idx, q, cut, hf, args, L, D):
     return nsparse.last_search_stats()
 
 
+def claim_order_launches(n_queries, device=None):
+    """1 when a batched search of n_queries runs the engine's claim-order
+    kernel before the search kernel (four or more queries per CTA; the
+    one-CTA-per-query kernel keeps four 8-warp CTAs per SM), else 0."""
+    import torch
+    dev = torch.cuda.current_device() if device is None else device
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    return 1 if n_queries >= 4 * min(n_queries, 4 * sms) else 0
+
+
 def replica_throughput(total_ms, e2e_s, n_queries, steps, e2e_steps, world, device=None):
     """Whole-job throughput of `world` replicas, each searching its own
     `n_queries` per step: every rank's time is replaced by the slowest rank's
@@ -481,7 +491,8 @@ def run_engine(args):
             "work": {"docs_scored_per_query": st.docs_scored / qs.n,
                      "unique_docs_scored_per_query": st_u.unique_docs / qs.n,
                      "blocks_visited_per_query": st.blocks_visited / qs.n},
-            "gpu_launches": args.steps,
+            # per step: the claim order and the search
+            "gpu_launches": args.steps * (1 + claim_order_launches(qs.n)),
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }
@@ -891,7 +902,9 @@ def run_engine_sq(args):
             "work": {"docs_scored_per_query": st.docs_scored / q1.n,
                      "unique_docs_scored_per_query": st_u.unique_docs / q1.n,
                      "blocks_visited_per_query": st.blocks_visited / q1.n},
-            "gpu_launches": args.steps * (2 * len(graphs) if graphs else len(bounds)),
+            # per batch: the query encode, the claim order and the search
+            "gpu_launches": args.steps * sum(2 + claim_order_launches(b1 - b0)
+                                             for b0, b1 in bounds),
             "clocks": clk.summary(),
         }
         if world == 1 and not args.no_cpu:
