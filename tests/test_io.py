@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 import nsparse
+from nsparse_b200 import synth
 import oracle as O
 from helpers import SEISMIC, golden_corpus, ref_file, ref_index, sq_spec
 
@@ -113,6 +114,24 @@ def test_quantized_add_writes_the_reference_codes(tmp_path, bits):
     vals[:4] = [-1.0, 0.0, 1e9, float(docs.values.max())]
     docs = type(docs)(docs.dim, docs.indptr, docs.indices, vals)
     vmin, vmax = 0.05, 9.5
+    spec = (f"seismic_sq,quantizer={bits}bit|vmin={vmin!r}|vmax={vmax!r}|"
+            "lambda=200|beta=20|alpha=0.4|seed=7")
+    ref_index(docs, spec, build=False).write(str(tmp_path / "r.idx"))
+    ours = nsparse.index_factory(docs.dim, spec)
+    ours.add(docs.n, docs.indptr, docs.indices, docs.values)
+    nsparse.write_index(ours, str(tmp_path / "o.idx"))
+    assert open(tmp_path / "o.idx", "rb").read() == open(tmp_path / "r.idx", "rb").read()
+
+
+@need_ref
+@pytest.mark.parametrize("bits", [8, 16])
+def test_quantized_add_of_a_large_batch_writes_the_reference_codes(tmp_path, bits):
+    """A batch of more than 4M values is encoded by several host threads (each
+    value on its own): the written index still equals the reference's byte
+    for byte."""
+    docs = synth.docs_config0(100_000, seed=5)  # ~13M values
+    assert docs.nnz > 3 * (1 << 22)
+    vmin, vmax = float(docs.values.min()), float(np.quantile(docs.values, 0.99))
     spec = (f"seismic_sq,quantizer={bits}bit|vmin={vmin!r}|vmax={vmax!r}|"
             "lambda=200|beta=20|alpha=0.4|seed=7")
     ref_index(docs, spec, build=False).write(str(tmp_path / "r.idx"))
